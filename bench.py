@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the per-step MHD hot path on B200.
+
+Metric: zone-cycles/s (one cell advanced by one full SSP-RK3 step) and the
+fraction of the measured HBM peak.  Default workload (one GPU): the MHD rotor,
+1024^2, outflow on every side, HLLE + MC + MOOD, plain FP64 -- the drop-in
+configuration.  Synthetic seeded / analytic initial states; no dataset.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl chimera|reference]
+
+N > 1 (launched by torch.distributed.run): every rank advances its own replica
+(the single-grid path does not shard; weak scaling, no data-path collective);
+timing is the max over ranks.  --impl reference times the reference algorithm's
+CPU implementation (the FP64 restatement, OpenMP on all host threads) on the
+same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_ZC_FP64 = 384      # 8 accesses x 6 fields x 8 B over the three stages
+STAGE_ACCESSES = {1: 12, 2: 18, 3: 18}   # field accesses per cell per stage launch
+WORKLOAD = "MHD rotor 1024x1024, outflow all sides, HLLE + MC + MOOD, gamma 1.4, FP64 plain"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=40)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=("chimera", "reference"), default="chimera")
+    p.add_argument("--n", type=int, default=1024, help="grid size (default: the rotor workload)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(key):
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary
+    (``profiles/*.md`` lines of the form ``traffic[<key>]: <bytes>``)."""
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for line in f:
+                m = re.match(r"\s*traffic\[(.+?)\]:\s*([0-9.eE+]+)", line)
+                if m and m.group(1) == key:
+                    return float(m.group(2))
+    return None
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_rate(n, steps, max_seconds=30.0):
+    """The CPU restatement of the reference (OpenMP, every loop, all host
+    threads) on the same workload: zone-cycles/s over a bounded sample."""
+    from chimera_b200 import problems
+    from oracle import oracle
+    oracle.build()
+    oracle.set_omp_mode(2)
+    cfg, st = problems.rotor(n)
+    cfg = cfg.replace(t_end=1e30)
+    s = oracle.State(st)
+    oracle.run(cfg, s, 1)                      # warm-up (page-in, thread start)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        oracle.run(cfg, s, 1)
+        done += 1
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    el = time.perf_counter() - t0
+    cores = oracle.max_threads()
+    oracle.set_omp_mode(0)
+    return n * n * done / el, cores, done, el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    rate, cores, done, el = cpu_reference_rate(args.n, max(1, args.steps))
+    line = {
+        "impl": "reference",
+        "metric": "zone-cycles/s", "value": rate, "unit": "zone-cycles/s", "n_gpus": args.gpus,
+        "steps": done, "warmup": 1, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("FP64 plain", "FP64, CPU"), "cells": args.n * args.n},
+        "cpu_baseline": {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "port",
+                         "sample": f"{done} RK3 steps of the {args.n}^2 rotor from t=0 (FP64 C restatement "
+                                   f"of the reference Fortran, OpenMP on every loop)"},
+        "e2e": {"value": rate, "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_chimera(args, world, rank, local):
+    import torch
+    from chimera_b200 import gpu, problems
+
+    torch.cuda.set_device(local)
+    n = args.n
+    cells = n * n
+    cfg, st = problems.rotor(n)
+    cfg = cfg.replace(t_end=1e30)     # keep stepping past t=0.15; per-step work is unchanged
+    s = gpu.Solver(cfg)
+    s.set_state(st)
+    ext = torch.cuda.ExternalStream(s.stream)
+    s.step(args.warmup)
+    torch.cuda.synchronize()
+
+    # --- device-resident throughput (inputs resident in HBM; the three state sets,
+    #     3 x 48 MB, exceed the 126 MB L2, so no flush is needed between steps)
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0.record(ext)
+    s.step(args.steps)
+    e1.record(ext)
+    e1.synchronize()
+    ck = clocks.stop()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = dist_max(e0.elapsed_time(e1), world)
+    d = s.diag()
+    if d["status"] != 0:
+        raise RuntimeError(f"device status {d['status']} after the timed steps")
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # --- per-kernel device time (CUDA events around each launch, eager path)
+    s.set_profiling(True)
+    s.get_profile(reset=True)
+    s.step(min(args.steps, 20))
+    prof = s.get_profile(reset=True)
+    s.set_profiling(False)
+    avg = {k: v["ms"] / v["launches"] for k, v in prof.items() if v["launches"]}
+    dom = max((k for k in avg if k.startswith("stage")), key=lambda k: avg[k])
+    kidx = int(dom[-1])
+    alg_bytes = STAGE_ACCESSES[kidx] * 8 * cells
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / (avg[dom] * 1e-3) / 1e9
+    traffic = profile_traffic(f"fp64_hlle_{dom}_rotor{n}")
+
+    # --- end to end through the C-ABI with host buffers: every step copies the
+    #     state in from pinned host memory, advances one step, copies it out.
+    e2e = None
+    if not args.no_e2e:
+        host_in = [torch.from_numpy(a).pin_memory() for a in st]
+        host_out = [torch.empty((n, n), dtype=torch.float64).pin_memory() for _ in range(6)]
+        k2 = max(3, min(args.steps, 20))
+        s2 = gpu.Solver(cfg)
+        for _ in range(2):
+            s2.set_state(host_in)
+            s2.step(1)
+            s2.get_state(out=host_out)
+        ext2 = torch.cuda.ExternalStream(s2.stream)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        f0.record(ext2)
+        for _ in range(k2):
+            s2.set_state(host_in)
+            s2.step(1)
+            s2.get_state(out=host_out)
+        f1.record(ext2)
+        f1.synchronize()
+        ms2 = dist_max(f0.elapsed_time(f1), world)
+        s2.close()
+        e2e = {"value": world * cells * k2 / (ms2 * 1e-3), "unit": "zone-cycles/s",
+               "h2d_bytes_per_step": 6 * 8 * cells, "d2h_bytes_per_step": 6 * 8 * cells,
+               "steps": k2, "mode": "state copied host->device and back around every RK3 step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, done, el = cpu_reference_rate(n, 4, max_seconds=20.0)
+        cpu = {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "port",
+               "sample": f"{done} RK3 steps of the {n}^2 rotor from t=0 on the host cores "
+                         f"(FP64 C restatement, OpenMP on every loop), {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "zone-cycles/s", "value": value, "unit": "zone-cycles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic rotor initial state)",
+            "config": {"workload": WORKLOAD, "cells": cells, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (3 state sets x 48 MB > 126 MB)",
+                       "hbm_fraction": value / world * BYTES_PER_ZC_FP64 / (hbm * 1e9),
+                       "bytes_per_zone_cycle": BYTES_PER_ZC_FP64},
+            "roofline": {"bound": "hbm", "kernel": f"stage_kernel<double,HLLE,{kidx}>",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "avg_launch_ms": avg[dom], "per_kernel_avg_ms": avg},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 3 * args.steps,
+            "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_chimera(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

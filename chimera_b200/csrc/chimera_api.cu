@@ -1,0 +1,617 @@
+// chimera_api.cu -- host runtime behind include/chimera_gpu.h.
+//
+// A handle is a batch of grid members (a single grid is a batch of one).  It
+// owns, per member, three sets of six state buffers in HBM (the state and two
+// RK stage scratch sets), the device-resident time-loop state (Control), the
+// per-tile reduction partials and the (member, tile) work list; the stage
+// kernels are launched persistently over that work list, one launch per RK
+// stage, optionally replayed from a captured CUDA graph.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "../../include/chimera_gpu.h"
+#include "chimera_types.h"
+#include "kernel_table.h"
+
+using namespace chimera;
+
+namespace {
+
+// ---- FP32-bulk conversion kernels (host <-> storage precision) ---------------
+__global__ void k_f64_to_f32(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
+  for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+    dst[k] = float(src[k]);
+}
+__global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
+  for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+    dst[k] = double(src[k]);
+}
+
+bool valid_bc(int b) { return b >= CHIMERA_BC_PERIODIC && b <= CHIMERA_BC_INFLOW; }
+
+}  // namespace
+
+struct chimera_handle {
+  int n = 0;
+  std::vector<chimera_cfg> cfg;
+  std::vector<Member> hm;            // host copies of the member descriptors
+  int riemann = 1, limiter = 2, slope = 1, mood = 1, precision = CHIMERA_FP64;
+  int counters = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  int num_sms = 148;
+  KernelSet ks{};
+  int grid_stage[3] = {0, 0, 0};
+  int grid_cfl = 0;
+  int total_tiles = 0;
+  Member* d_members = nullptr;
+  Control* d_ctl = nullptr;
+  double* d_part = nullptr;
+  int* d_tile_member = nullptr;
+  void* pool = nullptr;              // all state buffers
+  double* d_stage64 = nullptr;       // FP64 staging for FP32-bulk set/get
+  size_t max_cells = 0;
+  std::vector<bool> dt_valid;        // per member: Control::dt matches the state
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int graph_steps_request = 0;
+  // CUDA-event timing of each launch on the handle's stream (eager path only)
+  int profiling = 0;
+  struct Timed { int kind; cudaEvent_t a, b; };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> spare;
+  double prof_ms[4] = {0, 0, 0, 0};   // cfl, stage 1, stage 2, stage 3
+  long long prof_n[4] = {0, 0, 0, 0};
+};
+
+static int cuda_fail(cudaError_t e) {
+  (void)e;
+  cudaGetLastError();  // clear sticky-free errors
+  return CHIMERA_ERR_CUDA;
+}
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t _e = (call);                       \
+    if (_e != cudaSuccess) return cuda_fail(_e);   \
+  } while (0)
+
+static int validate_cfg(const chimera_cfg* c) {
+  if (!c) return CHIMERA_ERR_BAD_ARG;
+  if (c->nx < 4 || c->ny < 4) return CHIMERA_ERR_BAD_ARG;                 // N >= 4 (src/mhd_init.f90:208)
+  if ((long long)c->nx * c->ny > (1LL << 31)) return CHIMERA_ERR_TOO_LARGE;
+  if (!(c->dx > 0.0) || !(c->dy > 0.0) || !(c->gamma > 1.0)) return CHIMERA_ERR_BAD_ARG;
+  if (!(c->courant > 0.0) || !(c->t_out > 0.0)) return CHIMERA_ERR_BAD_ARG;
+  if (!valid_bc(c->bc_xlo) || !valid_bc(c->bc_xhi) || !valid_bc(c->bc_ylo) || !valid_bc(c->bc_yhi))
+    return CHIMERA_ERR_BAD_ARG;
+  // A side that wraps while its opposite side does not has no consistent
+  // ghost state; the reference accepts it but it is not supported here.
+  if ((c->bc_xlo == CHIMERA_BC_PERIODIC) != (c->bc_xhi == CHIMERA_BC_PERIODIC)) return CHIMERA_ERR_UNSUPPORTED;
+  if ((c->bc_ylo == CHIMERA_BC_PERIODIC) != (c->bc_yhi == CHIMERA_BC_PERIODIC)) return CHIMERA_ERR_UNSUPPORTED;
+  if (c->riemann < 1 || c->riemann > 3) return CHIMERA_ERR_BAD_ARG;
+  if (c->limiter < 1 || c->limiter > 2) return CHIMERA_ERR_BAD_ARG;
+  if (c->precision != CHIMERA_FP64 && c->precision != CHIMERA_FP32_BULK) return CHIMERA_ERR_BAD_ARG;
+  return CHIMERA_OK;
+}
+
+static cudaEvent_t take_event(chimera_handle* h) {
+  if (!h->spare.empty()) {
+    cudaEvent_t e = h->spare.back();
+    h->spare.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  return e;
+}
+
+static void harvest_profile(chimera_handle* h) {
+  for (auto& t : h->timed) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+      h->prof_ms[t.kind] += ms;
+      h->prof_n[t.kind] += 1;
+    }
+    cudaGetLastError();
+    h->spare.push_back(t.a);
+    h->spare.push_back(t.b);
+  }
+  h->timed.clear();
+}
+
+static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid);
+
+// kind: 0 = CFL kernel, 1..3 = stage kernels
+static int launch(chimera_handle* h, const KernelEntry& k, int grid, int kind) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(h->stream, &cs);
+  if (!h->profiling || cs != cudaStreamCaptureStatusNone) return launch_raw(h, k, grid);
+  if (h->timed.size() > 4096) harvest_profile(h);
+  cudaEvent_t a = take_event(h), b = take_event(h);
+  if (!a || !b) return launch_raw(h, k, grid);
+  cudaEventRecord(a, h->stream);
+  int rc = launch_raw(h, k, grid);
+  cudaEventRecord(b, h->stream);
+  h->timed.push_back({kind, a, b});
+  return rc;
+}
+
+static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid) {
+  StageArgs a;
+  a.members = h->d_members;
+  a.ctl = h->d_ctl;
+  a.partials = h->d_part;
+  a.tile_member = h->d_tile_member;
+  a.n_members = h->n;
+  a.total_tiles = h->total_tiles;
+  a.limiter = h->limiter;
+  a.slope_limiting = h->slope;
+  a.mood = h->mood;
+  a.counters = h->counters;
+  void* args[] = {&a};
+  CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.nt), args, k.smem, h->stream));
+  return CHIMERA_OK;
+}
+
+static int grid_for(chimera_handle* h, const KernelEntry& k) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.nt, k.smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  cudaGetLastError();
+  return std::max(1, std::min(h->total_tiles, per_sm * h->num_sms));
+}
+
+static int ensure_dt(chimera_handle* h) {
+  bool all = true;
+  for (int m = 0; m < h->n; ++m) all = all && h->dt_valid[m];
+  if (all) return CHIMERA_OK;
+  int rc = launch(h, h->ks.cfl, h->grid_cfl, 0);
+  if (rc) return rc;
+  for (int m = 0; m < h->n; ++m) h->dt_valid[m] = true;
+  return CHIMERA_OK;
+}
+
+static int one_step(chimera_handle* h) {
+  for (int s = 0; s < 3; ++s) {
+    int rc = launch(h, h->ks.stage[h->riemann - 1][s], h->grid_stage[s], s + 1);
+    if (rc) return rc;
+  }
+  return CHIMERA_OK;
+}
+
+static void drop_graph(chimera_handle* h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_steps = 0;
+}
+
+static int run_steps(chimera_handle* h, int nsteps) {
+  int rc = ensure_dt(h);
+  if (rc) return rc;
+  if (h->graph_steps_request > 0 && nsteps == h->graph_steps_request) {
+    if (!h->graph || h->graph_steps != nsteps) {
+      drop_graph(h);
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      int crc = CHIMERA_OK;
+      for (int s = 0; s < nsteps && crc == CHIMERA_OK; ++s) crc = one_step(h);
+      cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+      if (crc) { if (g) cudaGraphDestroy(g); return crc; }
+      if (e != cudaSuccess) return cuda_fail(e);
+      e = cudaGraphInstantiate(&h->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { h->graph = nullptr; return cuda_fail(e); }
+      h->graph_steps = nsteps;
+    }
+    CK(cudaGraphLaunch(h->graph, h->stream));
+    return CHIMERA_OK;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    rc = one_step(h);
+    if (rc) return rc;
+  }
+  return CHIMERA_OK;
+}
+
+static size_t cells_of(const chimera_cfg& c) { return size_t(c.nx) * size_t(c.ny); }
+
+extern "C" {
+
+int chimera_version(void) { return 10000; }
+
+const char* chimera_strerror(int code) {
+  switch (code) {
+    case CHIMERA_OK: return "ok";
+    case CHIMERA_ERR_BAD_ARG: return "invalid argument";
+    case CHIMERA_ERR_CUDA: return "CUDA runtime error";
+    case CHIMERA_ERR_NONFINITE: return "non-finite state reported by the device";
+    case CHIMERA_ERR_TIMEOUT: return "bounded device wait timed out";
+    case CHIMERA_ERR_UNSUPPORTED: return "configuration not supported on this path";
+    case CHIMERA_ERR_NO_DEVICE: return "no usable CUDA device";
+    case CHIMERA_ERR_NOMEM: return "device allocation failed";
+    case CHIMERA_ERR_TOO_LARGE: return "size exceeds capacity";
+    default: return "unknown error";
+  }
+}
+
+int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, chimera_handle** out) {
+  if (!out || !cfgs || n_members < 1) return CHIMERA_ERR_BAD_ARG;
+  *out = nullptr;
+  for (int m = 0; m < n_members; ++m) {
+    int rc = validate_cfg(&cfgs[m]);
+    if (rc) return rc;
+    const chimera_cfg& a = cfgs[0];
+    const chimera_cfg& b = cfgs[m];
+    if (a.riemann != b.riemann || a.limiter != b.limiter || a.use_slope_limiting != b.use_slope_limiting ||
+        a.mood != b.mood || a.precision != b.precision)
+      return CHIMERA_ERR_BAD_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) { cudaGetLastError(); return CHIMERA_ERR_NO_DEVICE; }
+  chimera_handle* h = new (std::nothrow) chimera_handle();
+  if (!h) return CHIMERA_ERR_NOMEM;
+  h->n = n_members;
+  h->cfg.assign(cfgs, cfgs + n_members);
+  h->riemann = cfgs[0].riemann;
+  h->limiter = cfgs[0].limiter;
+  h->slope = cfgs[0].use_slope_limiting ? 1 : 0;
+  h->mood = cfgs[0].mood ? 1 : 0;
+  h->precision = cfgs[0].precision;
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+  if (h->precision == CHIMERA_FP64) fp64_kernels(0, &h->ks);
+  else fp32_kernels(0, &h->ks);
+  for (int r = 0; r < 3; ++r)
+    for (int s = 0; s < 3; ++s)
+      cudaFuncSetAttribute(h->ks.stage[r][s].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(h->ks.stage[r][s].smem));
+  cudaGetLastError();
+  if (stream) {
+    h->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return CHIMERA_ERR_CUDA;
+    }
+    h->own_stream = true;
+  }
+  // members, work list
+  const int tx = h->ks.stage[0][0].tx, ty = h->ks.stage[0][0].ty;
+  const int eb = h->ks.elem_bytes;
+  h->hm.resize(n_members);
+  size_t pool_bytes = 0;
+  int tiles = 0;
+  for (int m = 0; m < n_members; ++m) {
+    const chimera_cfg& c = cfgs[m];
+    Member& g = h->hm[m];
+    memset(&g, 0, sizeof(g));
+    g.nx = c.nx; g.ny = c.ny;
+    g.tiles_x = (c.nx + tx - 1) / tx;
+    g.tiles_y = (c.ny + ty - 1) / ty;
+    g.tile_begin = tiles;
+    tiles += g.tiles_x * g.tiles_y;
+    g.periodic_x = c.bc_xlo == CHIMERA_BC_PERIODIC;
+    g.periodic_y = c.bc_ylo == CHIMERA_BC_PERIODIC;
+    g.square = (c.dx == c.dy) ? 1 : 0;
+    g.dx = c.dx; g.dy = c.dy;
+    g.inv_dx = 1.0 / c.dx; g.inv_dy = 1.0 / c.dy;
+    g.inv_2dx = 1.0 / (2.0 * c.dx); g.inv_2dy = 1.0 / (2.0 * c.dy);
+    g.hx = 0.5 * c.dx; g.hy = 0.5 * c.dy;
+    g.gamma = c.gamma;
+    g.vol = c.dx * c.dy;
+    g.len = (c.dx < c.dy) ? c.dx : c.dy;
+    g.courant = c.courant;
+    g.t_out = c.t_out;
+    g.t_end = c.t_end;
+    const size_t n = cells_of(c);
+    h->max_cells = std::max(h->max_cells, n);
+    pool_bytes += 18 * ((n * eb + 255) / 256) * 256;
+  }
+  h->total_tiles = tiles;
+  h->dt_valid.assign(n_members, false);
+  if (cudaMalloc(&h->pool, pool_bytes) != cudaSuccess) { cudaGetLastError(); chimera_destroy(h); return CHIMERA_ERR_NOMEM; }
+  cudaMemsetAsync(h->pool, 0, pool_bytes, h->stream);
+  char* p = (char*)h->pool;
+  for (int m = 0; m < n_members; ++m) {
+    const size_t fb = ((cells_of(cfgs[m]) * eb + 255) / 256) * 256;
+    for (int b = 0; b < 3; ++b)
+      for (int q = 0; q < 6; ++q) { h->hm[m].buf[b][q] = p; p += fb; }
+  }
+  std::vector<int> tm(tiles);
+  for (int m = 0; m < n_members; ++m)
+    for (int k = 0; k < h->hm[m].tiles_x * h->hm[m].tiles_y; ++k) tm[h->hm[m].tile_begin + k] = m;
+  std::vector<Control> ctl(n_members);
+  for (int m = 0; m < n_members; ++m) {
+    memset(&ctl[m], 0, sizeof(Control));
+    ctl[m].t = 0.0;
+    ctl[m].output_count = 1;
+    ctl[m].active = 1;
+  }
+  if (cudaMalloc(&h->d_members, sizeof(Member) * n_members) != cudaSuccess ||
+      cudaMalloc(&h->d_ctl, sizeof(Control) * n_members) != cudaSuccess ||
+      cudaMalloc(&h->d_part, sizeof(double) * NPART * size_t(tiles)) != cudaSuccess ||
+      cudaMalloc(&h->d_tile_member, sizeof(int) * size_t(tiles)) != cudaSuccess) {
+    cudaGetLastError();
+    chimera_destroy(h);
+    return CHIMERA_ERR_NOMEM;
+  }
+  if (h->precision == CHIMERA_FP32_BULK) {
+    if (cudaMalloc(&h->d_stage64, sizeof(double) * h->max_cells) != cudaSuccess) {
+      cudaGetLastError();
+      chimera_destroy(h);
+      return CHIMERA_ERR_NOMEM;
+    }
+  }
+  cudaMemcpyAsync(h->d_members, h->hm.data(), sizeof(Member) * n_members, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_ctl, ctl.data(), sizeof(Control) * n_members, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_tile_member, tm.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, h->stream);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) { cudaGetLastError(); chimera_destroy(h); return CHIMERA_ERR_CUDA; }
+  for (int s = 0; s < 3; ++s) h->grid_stage[s] = grid_for(h, h->ks.stage[h->riemann - 1][s]);
+  h->grid_cfl = grid_for(h, h->ks.cfl);
+  *out = h;
+  return CHIMERA_OK;
+}
+
+int chimera_create(const chimera_cfg* cfg, void* stream, chimera_handle** out) {
+  if (!cfg) return CHIMERA_ERR_BAD_ARG;
+  return chimera_batch_create(1, cfg, stream, out);
+}
+
+void chimera_destroy(chimera_handle* h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graph(h);
+  harvest_profile(h);
+  for (auto e : h->spare) cudaEventDestroy(e);
+  cudaFree(h->pool);
+  cudaFree(h->d_members);
+  cudaFree(h->d_ctl);
+  cudaFree(h->d_part);
+  cudaFree(h->d_tile_member);
+  cudaFree(h->d_stage64);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  cudaGetLastError();
+  delete h;
+}
+
+void* chimera_stream(chimera_handle* h) { return h ? (void*)h->stream : nullptr; }
+int chimera_batch_size(chimera_handle* h) { return h ? h->n : CHIMERA_ERR_BAD_ARG; }
+
+static int read_ctl(chimera_handle* h, int m, Control* c) {
+  CK(cudaMemcpyAsync(c, h->d_ctl + m, sizeof(Control), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return CHIMERA_OK;
+}
+
+// Copy one field between a caller array (ld pitch, host or device) and a
+// dense device buffer of the handle's storage precision.
+static int copy_field_in(chimera_handle* h, int m, void* dst, const double* src, int ld, int where) {
+  const chimera_cfg& c = h->cfg[m];
+  const size_t w = size_t(c.nx) * sizeof(double);
+  const cudaMemcpyKind kind = (where == CHIMERA_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  if (h->precision == CHIMERA_FP64) {
+    CK(cudaMemcpy2DAsync(dst, w, src, size_t(ld) * sizeof(double), w, c.ny, kind, h->stream));
+  } else {
+    CK(cudaMemcpy2DAsync(h->d_stage64, w, src, size_t(ld) * sizeof(double), w, c.ny, kind, h->stream));
+    const size_t n = cells_of(c);
+    k_f64_to_f32<<<h->num_sms * 4, 256, 0, h->stream>>>(h->d_stage64, (float*)dst, n);
+    CK(cudaGetLastError());
+  }
+  return CHIMERA_OK;
+}
+
+static int copy_field_out(chimera_handle* h, int m, double* dst, const void* src, int ld, int where) {
+  const chimera_cfg& c = h->cfg[m];
+  const size_t w = size_t(c.nx) * sizeof(double);
+  const cudaMemcpyKind kind = (where == CHIMERA_HOST) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  if (h->precision == CHIMERA_FP64) {
+    CK(cudaMemcpy2DAsync(dst, size_t(ld) * sizeof(double), src, w, w, c.ny, kind, h->stream));
+  } else {
+    const size_t n = cells_of(c);
+    k_f32_to_f64<<<h->num_sms * 4, 256, 0, h->stream>>>((const float*)src, h->d_stage64, n);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy2DAsync(dst, size_t(ld) * sizeof(double), h->d_stage64, w, w, c.ny, kind, h->stream));
+  }
+  return CHIMERA_OK;
+}
+
+static int check_io(chimera_handle* h, int m, const void* const* ptrs, int ld, int where) {
+  if (!h || m < 0 || m >= h->n) return CHIMERA_ERR_BAD_ARG;
+  if (where != CHIMERA_HOST && where != CHIMERA_DEVICE) return CHIMERA_ERR_BAD_ARG;
+  if (ld < h->cfg[m].nx) return CHIMERA_ERR_BAD_ARG;
+  for (int q = 0; q < 6; ++q)
+    if (!ptrs[q]) return CHIMERA_ERR_BAD_ARG;
+  return CHIMERA_OK;
+}
+
+int chimera_batch_set_state(chimera_handle* h, int m, const double* Mass, const double* Momx,
+                            const double* Momy, const double* Energy, const double* b_x,
+                            const double* b_y, int ld, int where) {
+  const void* ptrs[6] = {Mass, Momx, Momy, Energy, b_x, b_y};
+  int rc = check_io(h, m, ptrs, ld, where);
+  if (rc) return rc;
+  Control c;
+  rc = read_ctl(h, m, &c);
+  if (rc) return rc;
+  for (int q = 0; q < 6; ++q) {
+    rc = copy_field_in(h, m, h->hm[m].buf[c.parity][q], (const double*)ptrs[q], ld, where);
+    if (rc) return rc;
+  }
+  h->dt_valid[m] = false;
+  return CHIMERA_OK;
+}
+
+int chimera_set_state(chimera_handle* h, const double* Mass, const double* Momx, const double* Momy,
+                      const double* Energy, const double* b_x, const double* b_y, int ld, int where) {
+  return chimera_batch_set_state(h, 0, Mass, Momx, Momy, Energy, b_x, b_y, ld, where);
+}
+
+static int get_buffer(chimera_handle* h, int m, int which, double* const* ptrs, int ld, int where) {
+  const void* p6[6] = {ptrs[0], ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptrs[5]};
+  int rc = check_io(h, m, p6, ld, where);
+  if (rc) return rc;
+  Control c;
+  rc = read_ctl(h, m, &c);
+  if (rc) return rc;
+  const int b = (which == 0) ? c.parity : (which == 1 ? 1 - c.parity : 2);
+  for (int q = 0; q < 6; ++q) {
+    rc = copy_field_out(h, m, ptrs[q], h->hm[m].buf[b][q], ld, where);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return c.status ? CHIMERA_ERR_NONFINITE : CHIMERA_OK;
+}
+
+int chimera_batch_get_state(chimera_handle* h, int m, double* Mass, double* Momx, double* Momy,
+                            double* Energy, double* b_x, double* b_y, int ld, int where) {
+  double* p[6] = {Mass, Momx, Momy, Energy, b_x, b_y};
+  return get_buffer(h, m, 0, p, ld, where);
+}
+
+int chimera_get_state(chimera_handle* h, double* Mass, double* Momx, double* Momy, double* Energy,
+                      double* b_x, double* b_y, int ld, int where) {
+  return chimera_batch_get_state(h, 0, Mass, Momx, Momy, Energy, b_x, b_y, ld, where);
+}
+
+int chimera_get_stage_buffer(chimera_handle* h, int b, double* Mass, double* Momx, double* Momy,
+                             double* Energy, double* b_x, double* b_y, int ld, int where) {
+  if (b < 0 || b > 2) return CHIMERA_ERR_BAD_ARG;
+  double* p[6] = {Mass, Momx, Momy, Energy, b_x, b_y};
+  return get_buffer(h, 0, b, p, ld, where);
+}
+
+int chimera_batch_set_time(chimera_handle* h, int m, double t, int output_count) {
+  if (!h || m < 0 || m >= h->n || output_count < 1) return CHIMERA_ERR_BAD_ARG;
+  Control c;
+  int rc = read_ctl(h, m, &c);
+  if (rc) return rc;
+  c.t = t;
+  c.output_count = output_count;
+  c.active = (t < h->cfg[m].t_end) ? 1 : 0;
+  CK(cudaMemcpyAsync(h->d_ctl + m, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->dt_valid[m] = false;
+  return CHIMERA_OK;
+}
+
+int chimera_set_time(chimera_handle* h, double t, int output_count) {
+  return chimera_batch_set_time(h, 0, t, output_count);
+}
+
+int chimera_step(chimera_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return CHIMERA_ERR_BAD_ARG;
+  if (nsteps == 0) return CHIMERA_OK;
+  return run_steps(h, nsteps);
+}
+
+int chimera_set_graph_steps(chimera_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return CHIMERA_ERR_BAD_ARG;
+  h->graph_steps_request = nsteps;
+  if (nsteps == 0) drop_graph(h);
+  return CHIMERA_OK;
+}
+
+int chimera_advance(chimera_handle* h, int max_steps, int* steps_taken) {
+  if (!h || max_steps < 0) return CHIMERA_ERR_BAD_ARG;
+  std::vector<Control> c(h->n);
+  std::vector<unsigned long long> s0(h->n);
+  CK(cudaMemcpyAsync(c.data(), h->d_ctl, sizeof(Control) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int m = 0; m < h->n; ++m) s0[m] = c[m].steps;
+  int done = 0;
+  const int chunk = 16;
+  while (done < max_steps) {
+    const int k = std::min(chunk, max_steps - done);
+    int rc = run_steps(h, k);
+    if (rc) return rc;
+    done += k;
+    CK(cudaMemcpyAsync(c.data(), h->d_ctl, sizeof(Control) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    bool any = false;
+    for (int m = 0; m < h->n; ++m) any = any || c[m].active;
+    if (!any) break;
+  }
+  if (steps_taken) {
+    unsigned long long mx = 0;
+    for (int m = 0; m < h->n; ++m) mx = std::max(mx, c[m].steps - s0[m]);
+    *steps_taken = int(mx);
+  }
+  for (int m = 0; m < h->n; ++m)
+    if (c[m].status) return CHIMERA_ERR_NONFINITE;
+  return CHIMERA_OK;
+}
+
+int chimera_stage(chimera_handle* h, int k, double dt) {
+  if (!h || k < 1 || k > 3) return CHIMERA_ERR_BAD_ARG;
+  for (int m = 0; m < h->n; ++m) {
+    Control c;
+    int rc = read_ctl(h, m, &c);
+    if (rc) return rc;
+    c.dt = dt;
+    c.active = 1;
+    CK(cudaMemcpyAsync(h->d_ctl + m, &c, sizeof(Control), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->dt_valid[m] = false;
+  }
+  return launch(h, h->ks.stage[h->riemann - 1][k - 1], h->grid_stage[k - 1], k);
+}
+
+int chimera_batch_diag(chimera_handle* h, int m, chimera_diag_out* out) {
+  if (!h || !out || m < 0 || m >= h->n) return CHIMERA_ERR_BAD_ARG;
+  int rc = ensure_dt(h);
+  if (rc) return rc;
+  Control c;
+  rc = read_ctl(h, m, &c);
+  if (rc) return rc;
+  const chimera_cfg& cf = h->cfg[m];
+  out->t = c.t;
+  out->dt = c.dt;
+  out->output_count = c.output_count;
+  out->active = c.active;
+  out->steps = c.steps;
+  out->divb_max = c.divb_max;
+  out->divb_mean = c.divb_sum / double(cells_of(cf));
+  out->bmax = c.bmax;
+  out->divb_rel = (c.bmax > 0.0) ? c.divb_max * std::min(cf.dx, cf.dy) / c.bmax : 0.0;
+  out->mass = c.mass;
+  out->energy = c.energy;
+  out->cfl_speed = c.cfl_speed;
+  out->mood_resets = c.mood_resets;
+  out->floor_hits = c.floor_hits;
+  out->status = c.status;
+  return CHIMERA_OK;
+}
+
+int chimera_diag(chimera_handle* h, chimera_diag_out* out) { return chimera_batch_diag(h, 0, out); }
+
+int chimera_set_profiling(chimera_handle* h, int on) {
+  if (!h) return CHIMERA_ERR_BAD_ARG;
+  h->profiling = on ? 1 : 0;
+  return CHIMERA_OK;
+}
+
+int chimera_get_profile(chimera_handle* h, double* ms, long long* launches, int reset) {
+  if (!h || !ms || !launches) return CHIMERA_ERR_BAD_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  harvest_profile(h);
+  for (int k = 0; k < 4; ++k) {
+    ms[k] = h->prof_ms[k];
+    launches[k] = h->prof_n[k];
+    if (reset) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
+  }
+  return CHIMERA_OK;
+}
+
+int chimera_set_counters(chimera_handle* h, int on) {
+  if (!h) return CHIMERA_ERR_BAD_ARG;
+  h->counters = on ? 1 : 0;
+  drop_graph(h);
+  return CHIMERA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,58 @@
+// chimera_types.h -- device-resident descriptors shared by the host runtime
+// (chimera_api.cu) and the kernels.  Plain structs, no CUDA types.
+#pragma once
+#include <stdint.h>
+
+namespace chimera {
+
+constexpr int NPART = 6;  // per-tile partials: cfl speed max, |divB| max, |divB| sum, |B| max, mass, energy
+
+enum : unsigned {
+  STATUS_NONFINITE = 1u,   // a non-finite or non-positive quantity reached a reduction
+  STATUS_TIMEOUT = 2u,     // a bounded wait gave up
+  STATUS_BOUNDS = 4u,      // an index check failed (debug builds)
+};
+
+// One grid of the batch.  buf[b][q]: buffer b, field q; buffers 0 and 1
+// alternate as the state U^n and the stage-1 scratch U1 (Control::parity
+// says which holds the state), buffer 2 is the stage-2 scratch U2; field q (Mass, Momx, Momy, Energy, b_x, b_y), dense (ny, nx) with
+// x fastest, element type given by the handle's precision.
+struct Member {
+  int nx, ny;
+  int tiles_x, tiles_y;
+  int tile_begin;          // first global work-list index of this member
+  int periodic_x, periodic_y;
+  int square;              // dx == dy: the reference's single-spacing expressions apply
+  double dx, dy;
+  double inv_dx, inv_dy;   // 1/dx, 1/dy as the reference computes them
+  double inv_2dx, inv_2dy; // 1/(2 dx), 1/(2 dy)
+  double hx, hy;           // 0.5*dx, 0.5*dy
+  double gamma, vol, len;  // vol = dx*dy, len = min(dx, dy)
+  double courant, t_out, t_end;
+  void* buf[3][6];
+  void* e64[3];            // FP32-bulk form: FP64 Energy per buffer (unused in FP64)
+};
+
+// Time-loop state of one member, resident on the device so that whole runs
+// can be captured in a CUDA graph.
+struct Control {
+  double t, dt;
+  int output_count, active;
+  int parity, pad0;        // buf[parity] holds the current state
+  unsigned tiles_done, status;
+  unsigned long long steps, mood_resets, floor_hits;
+  double cfl_speed, divb_max, divb_sum, bmax, mass, energy;
+};
+
+struct StageArgs {
+  const Member* members;
+  Control* ctl;
+  double* partials;        // [total_tiles][NPART]
+  const int* tile_member;  // work index -> member (n_members > 1)
+  int n_members;
+  int total_tiles;
+  int limiter, slope_limiting, mood;
+  int counters;            // count MOOD resets / floor hits
+};
+
+}  // namespace chimera

@@ -1,0 +1,26 @@
+// kernel_table.h -- the instantiated kernels each precision unit exports to the
+// host runtime.
+#pragma once
+#include <stddef.h>
+
+namespace chimera {
+
+struct KernelEntry {
+  const void* fn;      // __global__ function (host stub address)
+  size_t smem;         // dynamic shared memory bytes
+  int tx, ty, nt;      // tile shape and block size
+};
+
+struct KernelSet {
+  KernelEntry stage[3][3];  // [riemann-1][stage-1]
+  KernelEntry cfl;
+  int elem_bytes;           // storage element size
+};
+
+// Tile-shape variants per precision (for the autotuner).
+int fp64_variant_count();
+void fp64_kernels(int variant, KernelSet* out);
+int fp32_variant_count();
+void fp32_kernels(int variant, KernelSet* out);
+
+}  // namespace chimera

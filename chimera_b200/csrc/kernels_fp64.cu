@@ -1,0 +1,33 @@
+// kernels_fp64.cu -- the plain FP64 form.  Compiled with --fmad=false so that
+// no multiply-add is contracted and every expression rounds as the reference's
+// Fortran source does (bit-compatible with the -ffp-contract=off restatement).
+#include "kernel_table.h"
+#include "stage_kernel.cuh"
+
+namespace chimera {
+
+namespace {
+template <int TX, int TY, int NT>
+void fill(KernelSet* ks) {
+  using G = TileGeom<TX, TY>;
+  const size_t smem = G::template smem_bytes<double>();
+#define CHIMERA_ENTRY(S, K) \
+  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel<double, S, K, TX, TY, NT>, smem, TX, TY, NT}
+  CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
+  CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
+  CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
+#undef CHIMERA_ENTRY
+  ks->cfl = KernelEntry{(const void*)&cfl_kernel<double, TX, TY, NT>, 0, TX, TY, NT};
+  ks->elem_bytes = 8;
+}
+}  // namespace
+
+int fp64_variant_count() { return 1; }
+
+void fp64_kernels(int variant, KernelSet* out) {
+  switch (variant) {
+    default: fill<32, 16, 256>(out); break;
+  }
+}
+
+}  // namespace chimera

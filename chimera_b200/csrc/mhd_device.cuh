@@ -1,0 +1,382 @@
+// mhd_device.cuh -- per-cell and per-face arithmetic of CHIMERA's stage operator.
+//
+// Templated on the arithmetic type R.  With R = double and the translation
+// unit compiled with --fmad=false, every expression below rounds exactly as
+// the Fortran source it cites (same operands, same left-to-right order, no
+// fused multiply-add), so the FP64 form is bit-compatible with the reference
+// semantics.  With R = float the same expressions run in FP32 (the FP32-bulk
+// form), with FMA contraction allowed.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace chimera {
+
+// src/mhd_config.f90:27-43
+enum { RIEMANN_RUSANOV = 1, RIEMANN_HLLE = 2, RIEMANN_HLLD = 3 };
+enum { LIMITER_VAN_LEER = 1, LIMITER_MC = 2 };
+enum { BC_PERIODIC = 1, BC_FIXED = 2, BC_OUTFLOW = 3, BC_INFLOW = 4 };
+
+template <typename R> struct K {
+  // src/mhd_config.f90:59-61
+  static constexpr R P_floor = R(1.0e-12);
+  static constexpr R rho_floor = R(1.0e-12);
+  static constexpr R e_floor_frac = R(1.0e-10);
+};
+
+template <typename R> __device__ __forceinline__ R dmax(R a, R b) { return (a > b) ? a : b; }
+template <typename R> __device__ __forceinline__ R dmin(R a, R b) { return (a < b) ? a : b; }
+template <typename R> __device__ __forceinline__ R dabs(R a) { return a < R(0) ? -a : a; }
+__device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ double dcopysign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ float dcopysign(float a, float b) { return copysignf(a, b); }
+__device__ __forceinline__ bool disfinite(double a) { return isfinite(a); }
+__device__ __forceinline__ bool disfinite(float a) { return isfinite(a); }
+
+// Primitive state of one cell: rho, vx, vy, P (TOTAL pressure), Bx, By.
+template <typename R> struct Prim {
+  R rho, vx, vy, P, Bx, By;
+};
+
+// src/mhd_change_states.f90:61-113 (get_primitive), one cell.
+template <typename R>
+__device__ __forceinline__ Prim<R> get_primitive(R M, R Mx, R My, R E, R Bx, R By, R gamma, R vol) {
+  Prim<R> p;
+  R r = dmax(M / vol, K<R>::rho_floor);
+  R u = Mx / (r * vol);
+  R v = My / (r * vol);
+  R halfB2 = R(0.5) * (Bx * Bx + By * By);
+  R P = ((E / vol - R(0.5) * r * (u * u + v * v)) - halfB2) * (gamma - R(1)) + halfB2;
+  P = dmax(P, K<R>::P_floor);
+  P = dmax(P, halfB2 + K<R>::e_floor_frac * (R(0.5) * r * (u * u + v * v) + halfB2));
+  p.rho = r; p.vx = u; p.vy = v; p.P = P; p.Bx = Bx; p.By = By;
+  return p;
+}
+
+// FP32-bulk form: the storage / bulk type is float but the pressure recovery
+// p = (gamma-1)(E - rho v^2/2 - B^2/2) + B^2/2 is done in FP64 (the
+// cancellation at low plasma beta), then rounded to float.
+__device__ __forceinline__ Prim<float> get_primitive_mixed(float M, float Mx, float My, double E,
+                                                           float Bx, float By, double gamma,
+                                                           double inv_vol) {
+  Prim<float> p;
+  float r = fmaxf(float(double(M) * inv_vol), 1.0e-12f);
+  float rv = float(double(r) / inv_vol);
+  float u = Mx / rv;
+  float v = My / rv;
+  double halfB2 = 0.5 * (double(Bx) * double(Bx) + double(By) * double(By));
+  double ke = 0.5 * double(r) * (double(u) * double(u) + double(v) * double(v));
+  double P = ((E * inv_vol - ke) - halfB2) * (gamma - 1.0) + halfB2;
+  P = fmax(P, 1.0e-12);
+  P = fmax(P, halfB2 + 1.0e-10 * (ke + halfB2));
+  p.rho = r; p.vx = u; p.vy = v; p.P = float(P); p.Bx = Bx; p.By = By;
+  return p;
+}
+
+// src/mhd_derivatives.f90:86-96 (apply_slope_limiter), one slope.
+template <typename R, int LIMITER>
+__device__ __forceinline__ R limit_slope(R dfL, R dfR) {
+  R prod = dfL * dfR;
+  R den = dfL + dfR;
+  if (prod <= R(0) || dabs(den) < R(1e-12)) return R(0);
+  if (LIMITER == LIMITER_VAN_LEER) return (R(2) * prod) / den;
+  return dcopysign(R(1), dfL) * dmin(dmin(R(2) * dabs(dfL), R(2) * dabs(dfR)), R(0.5) * dabs(den));
+}
+
+// Slope of cell c from its two neighbours: the limiter (useSlopeLimiting) or
+// the central difference of compute_gradients (src/mhd_derivatives.f90:44-45).
+template <typename R, int LIMITER, bool SLOPE>
+__device__ __forceinline__ R cell_slope(R fm, R f0, R fp, R inv_h, R inv_2h) {
+  if (SLOPE) return limit_slope<R, LIMITER>((f0 - fm) * inv_h, (fp - f0) * inv_h);
+  return (fp - fm) * inv_2h;
+}
+
+// One face's 5 fluxes in (normal, tangential) orientation.
+template <typename R> struct Flux5 {
+  R mass, momn, momt, energy, bt;
+};
+
+// src/mhd_flux.f90:197-288 (rusanov_flux), one interface.
+template <typename R>
+__device__ __forceinline__ Flux5<R> rusanov(R gamma, R rho_L, R rho_R, R vx_L, R vx_R, R vy_L, R vy_R,
+                                            R P_L, R P_R, R Bx_L, R Bx_R, R By_L, R By_R) {
+  Flux5<R> F;
+  R halfBL2 = R(0.5) * (Bx_L * Bx_L + By_L * By_L);
+  R halfBR2 = R(0.5) * (Bx_R * Bx_R + By_R * By_R);
+  R p_th_L = dmax(P_L - halfBL2, K<R>::P_floor);
+  R p_th_R = dmax(P_R - halfBR2, K<R>::P_floor);
+  R gm1 = gamma - R(1);
+  R en_L = (p_th_L / gm1 + R(0.5) * rho_L * (vx_L * vx_L + vy_L * vy_L)) + halfBL2;
+  R en_R = (p_th_R / gm1 + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
+  R rho_avg = R(0.5) * (rho_L + rho_R);
+  R inv_rho_avg = R(1) / rho_avg;
+  R momx_avg = R(0.5) * (rho_L * vx_L + rho_R * vx_R);
+  R momy_avg = R(0.5) * (rho_L * vy_L + rho_R * vy_R);
+  R en_avg = R(0.5) * (en_L + en_R);
+  R Bx_avg = R(0.5) * (Bx_L + Bx_R);
+  R By_avg = R(0.5) * (By_L + By_R);
+  R hB = R(0.5) * (Bx_avg * Bx_avg + By_avg * By_avg);
+  R P_avg = gm1 * ((en_avg - R(0.5) * (momx_avg * momx_avg + momy_avg * momy_avg) * inv_rho_avg) - hB) + hB;
+  F.mass = momx_avg;
+  F.momn = (momx_avg * momx_avg * inv_rho_avg + P_avg) - Bx_avg * Bx_avg;
+  F.momt = momx_avg * momy_avg * inv_rho_avg - Bx_avg * By_avg;
+  F.energy = (en_avg + P_avg) * momx_avg * inv_rho_avg - Bx_avg * (Bx_avg * momx_avg + By_avg * momy_avg) * inv_rho_avg;
+  F.bt = (By_avg * momx_avg - Bx_avg * momy_avg) * inv_rho_avg;
+  R c_L2 = (gamma * p_th_L + R(2) * halfBL2) / rho_L;
+  R c_R2 = (gamma * p_th_R + R(2) * halfBR2) / rho_R;
+  R C_L = dsqrt(R(0.5) * (c_L2 + dabs(c_L2))) + dabs(vx_L);
+  R C_R = dsqrt(R(0.5) * (c_R2 + dabs(c_R2))) + dabs(vx_R);
+  R C = R(0.5) * dmax(C_L, C_R);
+  F.mass = F.mass - C * (rho_R - rho_L);
+  F.momn = F.momn - C * (rho_R * vx_R - rho_L * vx_L);
+  F.momt = F.momt - C * (rho_R * vy_R - rho_L * vy_L);
+  F.energy = F.energy - C * (en_R - en_L);
+  F.bt = F.bt - C * (By_R - By_L);
+  return F;
+}
+
+// src/mhd_flux.f90:291-405 (hlle_flux), one interface.
+template <typename R>
+__device__ __forceinline__ Flux5<R> hlle(R gamma, R rho_L, R rho_R, R vx_L, R vx_R, R vy_L, R vy_R,
+                                         R P_L, R P_R, R Bx_L, R Bx_R, R By_L, R By_R) {
+  const R cf_max_hlle = R(1.0e2);
+  R halfBL2 = R(0.5) * (Bx_L * Bx_L + By_L * By_L);
+  R halfBR2 = R(0.5) * (Bx_R * Bx_R + By_R * By_R);
+  R p_th_L = dmax(P_L - halfBL2, K<R>::P_floor);
+  R p_th_R = dmax(P_R - halfBR2, K<R>::P_floor);
+  R gm1 = gamma - R(1);
+  R en_L = (p_th_L / gm1 + R(0.5) * rho_L * (vx_L * vx_L + vy_L * vy_L)) + halfBL2;
+  R en_R = (p_th_R / gm1 + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
+  R qL = (gamma * p_th_L + R(2) * halfBL2) / rho_L;
+  R qR = (gamma * p_th_R + R(2) * halfBR2) / rho_R;
+  R c_fL = dmin(dsqrt(R(0.5) * (qL + dabs(qL))), cf_max_hlle);
+  R c_fR = dmin(dsqrt(R(0.5) * (qR + dabs(qR))), cf_max_hlle);
+  R S_L = dmin(vx_L - c_fL, vx_R - c_fR);
+  R S_R = dmax(vx_L + c_fL, vx_R + c_fR);
+  R FL_Mass = rho_L * vx_L;
+  R FL_Momx = (rho_L * vx_L * vx_L + P_L) - Bx_L * Bx_L;
+  R FL_Momy = rho_L * vx_L * vy_L - Bx_L * By_L;
+  R FL_Energy = (en_L + P_L) * vx_L - Bx_L * (Bx_L * vx_L + By_L * vy_L);
+  R FL_By = By_L * vx_L - Bx_L * vy_L;
+  R FR_Mass = rho_R * vx_R;
+  R FR_Momx = (rho_R * vx_R * vx_R + P_R) - Bx_R * Bx_R;
+  R FR_Momy = rho_R * vx_R * vy_R - Bx_R * By_R;
+  R FR_Energy = (en_R + P_R) * vx_R - Bx_R * (Bx_R * vx_R + By_R * vy_R);
+  R FR_By = By_R * vx_R - Bx_R * vy_R;
+  Flux5<R> F;
+  if (S_L >= R(0)) {
+    F.mass = FL_Mass; F.momn = FL_Momx; F.momt = FL_Momy; F.energy = FL_Energy; F.bt = FL_By;
+  }
+  if (S_R <= R(0)) {
+    F.mass = FR_Mass; F.momn = FR_Momx; F.momt = FR_Momy; F.energy = FR_Energy; F.bt = FR_By;
+  }
+  if (!(S_L >= R(0)) && !(S_R <= R(0))) {
+    R inv_Sdiff = R(1) / dmax(S_R - S_L, R(1.0e-12));
+    R SLSR = S_L * S_R;
+    F.mass = ((S_R * FL_Mass - S_L * FR_Mass) + SLSR * (rho_R - rho_L)) * inv_Sdiff;
+    F.momn = ((S_R * FL_Momx - S_L * FR_Momx) + SLSR * (rho_R * vx_R - rho_L * vx_L)) * inv_Sdiff;
+    F.momt = ((S_R * FL_Momy - S_L * FR_Momy) + SLSR * (rho_R * vy_R - rho_L * vy_L)) * inv_Sdiff;
+    F.energy = ((S_R * FL_Energy - S_L * FR_Energy) + SLSR * (en_R - en_L)) * inv_Sdiff;
+    F.bt = ((S_R * FL_By - S_L * FR_By) + SLSR * (By_R - By_L)) * inv_Sdiff;
+  }
+  return F;
+}
+
+// HLL average of the two physical fluxes (src/mhd_flux.f90:595-600, 762-767).
+template <typename R>
+__device__ __forceinline__ Flux5<R> hll_avg(R SL, R SR, const Flux5<R>& FL, const Flux5<R>& FR,
+                                            R dM, R dMn, R dMt, R dE, R dB) {
+  Flux5<R> F;
+  R inv = R(1) / (SR - SL);
+  R s = SL * SR;
+  F.mass = ((SR * FL.mass - SL * FR.mass) + s * dM) * inv;
+  F.momn = ((SR * FL.momn - SL * FR.momn) + s * dMn) * inv;
+  F.momt = ((SR * FL.momt - SL * FR.momt) + s * dMt) * inv;
+  F.energy = ((SR * FL.energy - SL * FR.energy) + s * dE) * inv;
+  F.bt = ((SR * FL.bt - SL * FR.bt) + s * dB) * inv;
+  return F;
+}
+
+// src/mhd_flux.f90:408-779 (hlld_flux), one interface.
+template <typename R>
+__device__ __forceinline__ Flux5<R> hlld(R gamma, R rhoL, R rhoR, R vxL, R vxR, R vyL, R vyR,
+                                         R pTL, R pTR, R BxL, R BxR, R ByL, R ByR) {
+  const R EPS_FAN = R(1.0e-6);
+  const R FAC_BND = R(8.0);
+  const R cf_max_hlld = R(50.0);
+  R halfBL2 = R(0.5) * (BxL * BxL + ByL * ByL);
+  R halfBR2 = R(0.5) * (BxR * BxR + ByR * ByR);
+  R p_thL = dmax(pTL - halfBL2, K<R>::P_floor);
+  R p_thR = dmax(pTR - halfBR2, K<R>::P_floor);
+  R gm1 = gamma - R(1);
+  R enL = (p_thL / gm1 + R(0.5) * rhoL * (vxL * vxL + vyL * vyL)) + halfBL2;
+  R enR = (p_thR / gm1 + R(0.5) * rhoR * (vxR * vxR + vyR * vyR)) + halfBR2;
+
+  R vdotBL = vxL * BxL + vyL * ByL;
+  Flux5<R> FL, FR;
+  FL.mass = rhoL * vxL;
+  FL.momn = (rhoL * (vxL * vxL) + pTL) - BxL * BxL;
+  FL.momt = rhoL * vxL * vyL - BxL * ByL;
+  FL.energy = (enL + pTL) * vxL - BxL * vdotBL;
+  FL.bt = ByL * vxL - BxL * vyL;
+  R vdotBR = vxR * BxR + vyR * ByR;
+  FR.mass = rhoR * vxR;
+  FR.momn = (rhoR * (vxR * vxR) + pTR) - BxR * BxR;
+  FR.momt = rhoR * vxR * vyR - BxR * ByR;
+  FR.energy = (enR + pTR) * vxR - BxR * vdotBR;
+  FR.bt = ByR * vxR - BxR * vyR;
+
+  R caL = (BxL * BxL) / rhoL;
+  R caR = (BxR * BxR) / rhoR;
+  R csL2 = gamma * p_thL / rhoL;
+  R csR2 = gamma * p_thR / rhoR;
+  R b2L = (BxL * BxL + ByL * ByL) / rhoL;
+  R b2R = (BxR * BxR + ByR * ByR) / rhoR;
+  R tmpL = csL2 + b2L;
+  R tmpR = csR2 + b2R;
+  R cfL = dmin(dsqrt(R(0.5) * (tmpL + dsqrt(dmax(tmpL * tmpL - R(4) * csL2 * caL, R(0))))), cf_max_hlld);
+  R cfR = dmin(dsqrt(R(0.5) * (tmpR + dsqrt(dmax(tmpR * tmpR - R(4) * csR2 * caR, R(0))))), cf_max_hlld);
+  R SL = dmin(vxL - cfL, vxR - cfR);
+  R SR = dmax(vxL + cfL, vxR + cfR);
+
+  if (cfL >= cf_max_hlld || cfR >= cf_max_hlld) return (cfL <= cfR) ? FL : FR;   // :548-559
+  if (SL >= R(0)) return FL;                                                      // :562-567
+  if (SR <= R(0)) return FR;                                                      // :568-573
+
+  R dM = rhoR - rhoL;
+  R dMn = rhoR * vxR - rhoL * vxL;
+  R dMt = rhoR * vyR - rhoL * vyL;
+  R dE = enR - enL;
+  R dB = ByR - ByL;
+
+  R denMD = rhoR * (SR - vxR) - rhoL * (SL - vxL);
+  if (dabs(denMD) < R(1.0e-15)) denMD = dcopysign(R(1.0e-15), denMD);
+  R SM = ((rhoR * vxR * (SR - vxR) - rhoL * vxL * (SL - vxL)) - (pTR - pTL)) / denMD;
+  R pT_star = pTL + rhoL * (SL - vxL) * (SM - vxL);
+  if (SM <= SL + EPS_FAN * (SR - SL) || SM >= SR - EPS_FAN * (SR - SL))          // :594-602
+    return hll_avg(SL, SR, FL, FR, dM, dMn, dMt, dE, dB);
+  pT_star = dmax(pT_star, K<R>::P_floor);
+
+  R rho_Ls = rhoL * (SL - vxL) / (SL - SM);
+  R denL = rhoL * (SL - vxL) * (SL - SM) - BxL * BxL;
+  R vy_Ls, By_Ls;
+  if (dabs(denL) > R(1.0e-3) * dmax(dmax(dabs(rhoL * (SL - vxL) * (SL - SM)), BxL * BxL), R(1.0e-30))) {
+    vy_Ls = vyL - BxL * ByL * (SM - vxL) / denL;
+    By_Ls = ByL * (rhoL * ((SL - vxL) * (SL - vxL)) - BxL * BxL) / denL;
+  } else {
+    vy_Ls = vyL; By_Ls = ByL;
+  }
+  R vdotBLs = SM * BxL + vy_Ls * By_Ls;
+  R en_Ls = (((enL * (SL - vxL) - pTL * vxL) + pT_star * SM) + BxL * (vdotBL - vdotBLs)) / (SL - SM);
+
+  R rho_Rs = rhoR * (SR - vxR) / (SR - SM);
+  R denR = rhoR * (SR - vxR) * (SR - SM) - BxR * BxR;
+  R vy_Rs, By_Rs;
+  if (dabs(denR) > R(1.0e-3) * dmax(dmax(dabs(rhoR * (SR - vxR) * (SR - SM)), BxR * BxR), R(1.0e-30))) {
+    vy_Rs = vyR - BxR * ByR * (SM - vxR) / denR;
+    By_Rs = ByR * (rhoR * ((SR - vxR) * (SR - vxR)) - BxR * BxR) / denR;
+  } else {
+    vy_Rs = vyR; By_Rs = ByR;
+  }
+  R vdotBRs = SM * BxR + vy_Rs * By_Rs;
+  R en_Rs = (((enR * (SR - vxR) - pTR * vxR) + pT_star * SM) + BxR * (vdotBR - vdotBRs)) / (SR - SM);
+
+  R SqrtRhoLs = dsqrt(dmax(rho_Ls, K<R>::rho_floor));
+  R SqrtRhoRs = dsqrt(dmax(rho_Rs, K<R>::rho_floor));
+  R Bx_avg = R(0.5) * (BxL + BxR);
+  R SLs = SM - dabs(Bx_avg) / SqrtRhoLs;
+  R SRs = SM + dabs(Bx_avg) / SqrtRhoRs;
+  R vy_ss, By_ss, en_Lss, en_Rss;
+  if (dabs(Bx_avg) > R(1.0e-10)) {
+    R signBx = dcopysign(R(1), Bx_avg);
+    R denom_ss = SqrtRhoLs + SqrtRhoRs;
+    vy_ss = ((SqrtRhoLs * vy_Ls + SqrtRhoRs * vy_Rs) + signBx * (By_Rs - By_Ls)) / denom_ss;
+    By_ss = ((SqrtRhoLs * By_Rs + SqrtRhoRs * By_Ls) + signBx * SqrtRhoLs * SqrtRhoRs * (vy_Rs - vy_Ls)) / denom_ss;
+    R vdotBss = SM * Bx_avg + vy_ss * By_ss;
+    en_Lss = en_Ls - SqrtRhoLs * signBx * (vdotBLs - vdotBss);
+    en_Rss = en_Rs + SqrtRhoRs * signBx * (vdotBRs - vdotBss);
+  } else {
+    vy_ss = R(0.5) * (vy_Ls + vy_Rs);
+    By_ss = R(0.5) * (By_Ls + By_Rs);
+    en_Lss = en_Ls;
+    en_Rss = en_Rs;
+    SLs = SM;
+    SRs = SM;
+  }
+
+  Flux5<R> F;
+  if (SM >= R(0)) {
+    F.mass = FL.mass + SL * (rho_Ls - rhoL);
+    F.momn = FL.momn + SL * (rho_Ls * SM - rhoL * vxL);
+    F.momt = FL.momt + SL * (rho_Ls * vy_Ls - rhoL * vyL);
+    F.energy = FL.energy + SL * (en_Ls - enL);
+    F.bt = FL.bt + SL * (By_Ls - ByL);
+    if (!(SLs >= R(0))) {
+      F.momt = F.momt + SLs * rho_Ls * (vy_ss - vy_Ls);
+      F.energy = F.energy + SLs * (en_Lss - en_Ls);
+      F.bt = F.bt + SLs * (By_ss - By_Ls);
+    }
+  } else {
+    F.mass = FR.mass + SR * (rho_Rs - rhoR);
+    F.momn = FR.momn + SR * (rho_Rs * SM - rhoR * vxR);
+    F.momt = FR.momt + SR * (rho_Rs * vy_Rs - rhoR * vyR);
+    F.energy = FR.energy + SR * (en_Rs - enR);
+    F.bt = FR.bt + SR * (By_Rs - ByR);
+    if (!(SRs <= R(0))) {
+      F.momt = F.momt + SRs * rho_Rs * (vy_ss - vy_Rs);
+      F.energy = F.energy + SRs * (en_Rss - en_Rs);
+      F.bt = F.bt + SRs * (By_ss - By_Rs);
+    }
+  }
+
+  // catch-all guard :747-768
+  R Smax = dmax(dabs(SL), dabs(SR));
+  R bnd_mass = dmax(dabs(FL.mass), dabs(FR.mass)) + Smax * (rhoL + rhoR);
+  R bnd_momx = dmax(dabs(FL.momn), dabs(FR.momn)) + Smax * (dabs(rhoL * vxL) + dabs(rhoR * vxR));
+  R bnd_momy = dmax(dabs(FL.momt), dabs(FR.momt)) + Smax * (dabs(rhoL * vyL) + dabs(rhoR * vyR));
+  R bnd_enr = dmax(dabs(FL.energy), dabs(FR.energy)) + Smax * (dabs(enL) + dabs(enR));
+  R bnd_by = dmax(dabs(FL.bt), dabs(FR.bt)) + Smax * (dabs(ByL) + dabs(ByR));
+  bool use_hll = false;
+  if (!disfinite(F.mass) || dabs(F.mass) > FAC_BND * bnd_mass) use_hll = true;
+  if (!disfinite(F.momn) || dabs(F.momn) > FAC_BND * bnd_momx) use_hll = true;
+  if (!disfinite(F.momt) || dabs(F.momt) > FAC_BND * bnd_momy) use_hll = true;
+  if (!disfinite(F.energy) || dabs(F.energy) > FAC_BND * bnd_enr) use_hll = true;
+  if (!disfinite(F.bt) || dabs(F.bt) > FAC_BND * bnd_by) use_hll = true;
+  if (use_hll) F = hll_avg(SL, SR, FL, FR, dM, dMn, dMt, dE, dB);
+  return F;
+}
+
+template <typename R, int SOLVER>
+__device__ __forceinline__ Flux5<R> riemann(R gamma, R rL, R rR, R uL, R uR, R vL, R vR, R PL, R PR,
+                                            R BnL, R BnR, R BtL, R BtR) {
+  if (SOLVER == RIEMANN_RUSANOV) return rusanov<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR);
+  if (SOLVER == RIEMANN_HLLE) return hlle<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR);
+  return hlld<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR);
+}
+
+// src/mhd_change_states.f90:116-166 (apply_conserved_floors), one cell.
+// Returns a bit mask: 1 = mass floor hit, 2 = velocity cap hit.
+template <typename R>
+__device__ __forceinline__ int conserved_floors(R& M, R& Mx, R& My, R& E, R Bx, R By, R gamma, R vol) {
+  int hit = 0;
+  R halfB2 = R(0.5) * (Bx * Bx + By * By);
+  if (M < K<R>::rho_floor * vol) {
+    Mx = R(0);
+    My = R(0);
+    M = K<R>::rho_floor * vol;
+    E = dmax(E, (K<R>::P_floor / (gamma - R(1)) + halfB2) * vol);
+    hit |= 1;
+  }
+  R mag = dsqrt(Mx * Mx + My * My);
+  R v_mag = mag / M;
+  if (v_mag > R(50)) {
+    R scale = R(50) * M / mag;
+    Mx = Mx * scale;
+    My = My * scale;
+    hit |= 2;
+  }
+  return hit;
+}
+
+}  // namespace chimera

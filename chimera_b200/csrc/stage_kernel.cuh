@@ -1,0 +1,551 @@
+// stage_kernel.cuh -- the fused SSP-RK3 stage kernel and the CFL kernel.
+//
+// One CTA handles one TX x TY tile of output cells of one grid member (a
+// persistent grid-stride loop over a work list of (member, tile)):
+//
+//   phase 1  primitives (rho, vx, vy, P_total, Bx, By) on the tile plus a
+//            2-cell halo, computed straight from the conserved state in HBM
+//            (coalesced loads; boundary conditions are index maps, so no ghost
+//            arrays are materialised) -> shared memory
+//   phase 2  every x- and y-face flux the tile needs: limited slopes, MUSCL
+//            face states, MOOD bounds check, face floors, thermal-pressure
+//            check, Riemann solver -> shared memory (each face once)
+//   phase 3a constrained transport: corner Ez from the face fluxes, curl,
+//            face-B update (+ RK blend) -> shared memory
+//   phase 3b cell update: flux divergence (x pass then y pass), conserved
+//            floors, outflow boundary correction, RK blend, floors -> HBM
+//   stage 3  epilogue: primitives of the new state, CFL speed, div B, |B|,
+//            totals -> per-tile partials; the last tile of a member reduces
+//            them in a fixed order and advances t, outputCount and dt.
+//
+// Each step of a phase cites the reference routine it restates.
+#pragma once
+#include "mhd_device.cuh"
+#include "chimera_types.h"
+
+namespace chimera {
+
+// Work-list / member descriptors (device side), see chimera_types.h.
+
+// Source cell of a (possibly out-of-domain) tile position: periodic wrap or
+// the nearest cell.  Positions of a ragged last tile can lie more than one
+// period beyond a small grid, so the wrap is a true modulo.
+__device__ __forceinline__ int map_index(int g, int n, int periodic) {
+  if (g >= 0 && g < n) return g;
+  if (periodic) {
+    int r = g % n;
+    return r < 0 ? r + n : r;
+  }
+  return g < 0 ? 0 : n - 1;
+}
+
+template <typename R> struct StageTileSmem;
+
+template <int TX, int TY> struct TileGeom {
+  static constexpr int PX = TX + 4, PY = TY + 4, NP = PX * PY;
+  static constexpr int FXW = TX + 1, FXH = TY + 2, NFX = FXW * FXH;   // x faces i in [i0-1,i0+TX), j in [j0-1,j0+TY+1)
+  static constexpr int FYW = TX + 2, FYH = TY + 1, NFY = FYW * FYH;   // y faces i in [i0-1,i0+TX+1), j in [j0-1,j0+TY)
+  static constexpr int BXW = TX + 1, NBX = BXW * TY;                  // new b_x: i in [i0-1,i0+TX), j in tile
+  static constexpr int BYW = TX, NBY = BYW * (TY + 1);                // new b_y: i in tile, j in [j0-1,j0+TY)
+  template <typename R> static constexpr size_t smem_bytes() {
+    return sizeof(R) * (size_t(6) * NP + size_t(5) * NFX + size_t(5) * NFY + NBX + NBY);
+  }
+};
+
+// Block-wide reductions (deterministic for a fixed block size).
+template <int NT>
+__device__ __forceinline__ double block_reduce_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NT / 32; ++k) r += red[k];
+  }
+  return r;  // valid on thread 0
+}
+
+template <int NT>
+__device__ __forceinline__ double block_reduce_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    r = red[0];
+    for (int k = 1; k < NT / 32; ++k) r = fmax(r, red[k]);
+  }
+  return r;
+}
+
+// Per-cell CFL speed cf + |v| (src/main.f90:72-79), FP64.
+__device__ __forceinline__ double cfl_speed(double rho, double vx, double vy, double P, double Bx,
+                                            double By, double gamma) {
+  double inv_rho = 1.0 / rho;
+  double c0_sq = gamma * (P - 0.5 * (Bx * Bx + By * By)) * inv_rho;
+  double ca_sq = (Bx * Bx + By * By) * inv_rho;
+  double cf = sqrt(c0_sq + ca_sq);
+  if (rho < 1.0e-3) cf = fmin(cf, 50.0);
+  return cf + sqrt(vx * vx + vy * vy);
+}
+
+// divB of one cell from face values (src/mhd_field_ops.f90:60-117).
+__device__ __forceinline__ double divb_cell(double bx, double bxm, double by, double bym, bool has_x,
+                                            bool has_y, double inv_dx, double inv_dy, bool square) {
+  if (square) {
+    if (has_x && has_y) return (((bx - bxm) + by) - bym) * inv_dx;
+    if (has_x) return (bx - bxm) * inv_dx;
+    if (has_y) return (by - bym) * inv_dx;
+    return 0.0;
+  }
+  if (has_x && has_y) return (bx - bxm) * inv_dx + (by - bym) * inv_dy;
+  if (has_x) return (bx - bxm) * inv_dx;
+  if (has_y) return (by - bym) * inv_dy;
+  return 0.0;
+}
+
+// Finish of one member's step, run by the CTA that completed its last tile:
+// fixed-order reduction of the tile partials, then the time-loop bookkeeping
+// of src/main.f90:72-83 and :273-292.
+template <int NT>
+__device__ void member_finish(const Member& g, Control* ctl, const double* part, int ntiles,
+                              bool advance_time, double* red) {
+  double sp = 0.0, dmx = 0.0, dsum = 0.0, bmx = 0.0, ms = 0.0, es = 0.0;
+  for (int k = threadIdx.x; k < ntiles; k += NT) {
+    const double* p = part + size_t(g.tile_begin + k) * NPART;
+    sp = fmax(sp, __ldcg(p + 0));
+    dmx = fmax(dmx, __ldcg(p + 1));
+    dsum += __ldcg(p + 2);
+    bmx = fmax(bmx, __ldcg(p + 3));
+    ms += __ldcg(p + 4);
+    es += __ldcg(p + 5);
+  }
+  sp = block_reduce_max<NT>(sp, red);
+  dmx = block_reduce_max<NT>(dmx, red);
+  dsum = block_reduce_sum<NT>(dsum, red);
+  bmx = block_reduce_max<NT>(bmx, red);
+  ms = block_reduce_sum<NT>(ms, red);
+  es = block_reduce_sum<NT>(es, red);
+  if (threadIdx.x == 0) {
+    double t = ctl->t;
+    int oc = ctl->output_count;
+    if (advance_time) {
+      t = t + ctl->dt;                                           // src/main.f90:273
+      if (t >= double(oc) * g.t_out || t >= g.t_end) oc += 1;    // src/main.f90:279,291
+      ctl->steps += 1;
+      ctl->parity = 1 - ctl->parity;                             // U^{n+1} now in the other buffer
+    }
+    // src/main.f90:79: courant * minval(len / speed) == courant * (len / maxval(speed))
+    // because correctly rounded division is monotone in the divisor.
+    double dt = g.courant * (g.len / sp);
+    if (t + dt > double(oc) * g.t_out) dt = double(oc) * g.t_out - t;   // :82
+    dt = fmax(dt, double(1e-12f));                                       // :83 (single-precision literal)
+    ctl->t = t;
+    ctl->output_count = oc;
+    ctl->dt = dt;
+    ctl->active = (t < g.t_end) ? 1 : 0;
+    ctl->cfl_speed = sp;
+    ctl->divb_max = dmx;
+    ctl->divb_sum = dsum;
+    ctl->bmax = bmx;
+    ctl->mass = ms;
+    ctl->energy = es;
+    ctl->tiles_done = 0u;
+    if (!(sp > 0.0) || !isfinite(ms) || !isfinite(es)) atomicOr(&ctl->status, STATUS_NONFINITE);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// The fused stage kernel.
+// Buffers rotate through a device-resident parity bit: S = buf[parity] holds
+// U^n, O = buf[1 - parity] and buf[2] are scratch.
+//   STAGE 1: in = S (U^n), out = O (U1)
+//   STAGE 2: in = O, u0 = S, out = buf[2] (U2)
+//   STAGE 3: in = buf[2], u0 = S, out = O (U^{n+1}); the member finish flips
+//            the parity.  (Writing U^{n+1} over U^n in place would race: the
+//            epilogue's halo faces read U^n at the neighbour tile's cells.)
+// ----------------------------------------------------------------------------
+template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) stage_kernel(StageArgs a) {
+  using G = TileGeom<TX, TY>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sP = reinterpret_cast<R*>(smem_raw);
+  R* sFx = sP + 6 * G::NP;
+  R* sFy = sFx + 5 * G::NFX;
+  R* sBx = sFy + 5 * G::NFY;
+  R* sBy = sBx + G::NBX;
+  __shared__ double red[NT / 32];
+  __shared__ int s_last;
+
+  const int tid = threadIdx.x;
+  const bool slope_on = a.slope_limiting != 0;
+  const bool mood_on = a.mood != 0;
+  const bool van_leer = a.limiter == LIMITER_VAN_LEER;
+
+  for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
+    const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
+    const Member& g = a.members[m];
+    Control* ctl = a.ctl + m;
+    if (ctl->active == 0) continue;  // uniform across the CTA
+    const int nx = g.nx, ny = g.ny;
+    const int px = g.periodic_x, py = g.periodic_y;
+    const int lt = w - g.tile_begin;
+    const int i0 = (lt % g.tiles_x) * TX;
+    const int j0 = (lt / g.tiles_x) * TY;
+    const R gamma = R(g.gamma);
+    const R vol = R(g.vol);
+    const R dt = R(ctl->dt);
+    const int sbuf = ctl->parity, obuf = 1 - sbuf;
+    const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
+    const int out_buf = (STAGE == 2) ? 2 : obuf;
+    const R* __restrict__ in[6];
+    const R* __restrict__ u0[6];
+    R* __restrict__ out[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
+      u0[q] = reinterpret_cast<const R*>(g.buf[sbuf][q]);
+      out[q] = reinterpret_cast<R*>(g.buf[out_buf][q]);
+    }
+
+    // ---- phase 1: primitives on the tile + 2-cell halo ---------------------
+    // average_face_to_cell_B (src/mhd_field_ops.f90:120-156) + get_primitive
+    // (src/mhd_change_states.f90:61-113).  Out-of-domain positions take the
+    // primitive of the cell that fill_ghost_cells would copy there
+    // (src/mhd_bc.f90:36-121): wrap if periodic, else the nearest cell.
+    for (int p = tid; p < G::NP; p += NT) {
+      const int qx = p % G::PX, qy = p / G::PX;
+      const int si = map_index(i0 - 2 + qx, nx, px);
+      const int sj = map_index(j0 - 2 + qy, ny, py);
+      const size_t idx = size_t(sj) * nx + si;
+      const R bxc = in[4][idx];
+      const R byc = in[5][idx];
+      R Bx, By;
+      if (si > 0) Bx = R(0.5) * (bxc + in[4][idx - 1]);
+      else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
+      if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
+      else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
+      Prim<R> pr = get_primitive<R>(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, gamma, vol);
+      sP[0 * G::NP + p] = pr.rho;
+      sP[1 * G::NP + p] = pr.vx;
+      sP[2 * G::NP + p] = pr.vy;
+      sP[3 * G::NP + p] = pr.P;
+      sP[4 * G::NP + p] = pr.Bx;
+      sP[5 * G::NP + p] = pr.By;
+    }
+    __syncthreads();
+
+    // ---- phase 2: face fluxes ------------------------------------------------
+    unsigned mood_resets = 0;
+    for (int f = tid; f < G::NFX + G::NFY; f += NT) {
+      const bool ydir = f >= G::NFX;
+      const int ff = ydir ? f - G::NFX : f;
+      const int W = ydir ? G::FYW : G::FXW;
+      const int li = ff % W, lj = ff / W;
+      const int pa = (lj + 1) * G::PX + (li + 1);    // cell on the low side of the face
+      const int on = ydir ? G::PX : 1;               // offset along the face normal
+      const R inv_h = R(ydir ? g.inv_dy : g.inv_dx);
+      const R inv_2h = R(ydir ? g.inv_2dy : g.inv_2dx);
+      const R hh = R(ydir ? g.hy : g.hx);             // 0.5 * spacing
+      R L[6], Rv[6], C0[6];
+      bool reset = false;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const R* s = sP + q * G::NP;
+        const R fm = s[pa - on], f0 = s[pa], fp = s[pa + on], fpp = s[pa + 2 * on];
+        // apply_slope_limiter (src/mhd_derivatives.f90:50-127) or compute_gradients (:15-47)
+        R sa, sb;
+        if (slope_on) {
+          if (van_leer) {
+            sa = limit_slope<R, LIMITER_VAN_LEER>((f0 - fm) * inv_h, (fp - f0) * inv_h);
+            sb = limit_slope<R, LIMITER_VAN_LEER>((fp - f0) * inv_h, (fpp - fp) * inv_h);
+          } else {
+            sa = limit_slope<R, LIMITER_MC>((f0 - fm) * inv_h, (fp - f0) * inv_h);
+            sb = limit_slope<R, LIMITER_MC>((fp - f0) * inv_h, (fpp - fp) * inv_h);
+          }
+        } else {
+          sa = (fp - fm) * inv_2h;
+          sb = (fpp - f0) * inv_2h;
+        }
+        // reconstruction (src/mhd_derivatives.f90:160-182): left state from the low
+        // cell, right state = the high cell extrapolated back (temp_x(i+1)).
+        R vL = f0 + hh * sa;
+        R vR = fp - hh * sb;
+        const bool rp = (q == 0 || q == 3);
+        if (mood_on) {
+          // MOOD bounds of the LOW cell (:190-216), applied to both states and
+          // resetting both to the low cell's value (the reference's XR/YR rule).
+          R lo = dmin(dmin(dmin(dmin(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
+          const R hi = dmax(dmax(dmax(dmax(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
+          if (rp) lo = dmax(R(0.1e-8), lo);
+          if (vL < lo || vL > hi) { vL = f0; reset = true; }
+          if (vR < lo || vR > hi) { vR = f0; reset = true; }
+        }
+        if (rp) {                      // face floors (:223-227)
+          vL = dmax(vL, R(1.0e-8));
+          vR = dmax(vR, R(1.0e-8));
+        }
+        L[q] = vL; Rv[q] = vR; C0[q] = f0;
+      }
+      // thermal_pressure_check (src/mhd_derivatives.f90:232-293): reset all six
+      // fields of a face slot to the low cell's values.
+      if (L[3] - R(0.5) * (L[4] * L[4] + L[5] * L[5]) < K<R>::P_floor) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) L[q] = C0[q];
+      }
+      if (Rv[3] - R(0.5) * (Rv[4] * Rv[4] + Rv[5] * Rv[5]) < K<R>::P_floor) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) Rv[q] = C0[q];
+      }
+      mood_resets += reset ? 1u : 0u;
+      // compute_fluxes, rotated for y faces (src/main.f90:394-401)
+      const R unL = ydir ? L[2] : L[1], unR = ydir ? Rv[2] : Rv[1];
+      const R utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
+      const R bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
+      const R btL = ydir ? L[4] : L[5], btR = ydir ? Rv[4] : Rv[5];
+      Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
+      R* dst = ydir ? sFy : sFx;
+      const int NF = ydir ? G::NFY : G::NFX;
+      dst[0 * NF + ff] = F.mass;
+      dst[1 * NF + ff] = ydir ? F.momt : F.momn;   // x momentum flux
+      dst[2 * NF + ff] = ydir ? F.momn : F.momt;   // y momentum flux
+      dst[3 * NF + ff] = F.energy;
+      dst[4 * NF + ff] = F.bt;                     // By flux (x faces) / Bx flux (y faces)
+    }
+    if (a.counters) {
+      unsigned s = __reduce_add_sync(0xffffffffu, mood_resets);
+      if ((tid & 31) == 0 && s) atomicAdd(&ctl->mood_resets, (unsigned long long)s);
+    }
+    __syncthreads();
+
+    // ---- phase 3a: constrained transport -> new face B ------------------------
+    // constrained_transport (src/mhd_flux.f90:79-136) + compute_curl_2d(-Ez)
+    // (src/mhd_field_ops.f90:15-57), then the RK blend of b_x, b_y.
+    const R* FByX = sFx + 4 * G::NFX;
+    const R* FBxY = sFy + 4 * G::NFY;
+    auto Ez = [&](int ci, int cj) -> R {
+      const int xi = (cj - j0 + 1) * G::FXW + (ci - i0 + 1);
+      const R fa = FByX[xi];
+      const R up = (cj == ny - 1 && !py) ? fa : FByX[xi + G::FXW];
+      const int yi = (cj - j0 + 1) * G::FYW + (ci - i0 + 1);
+      const R fb = FBxY[yi];
+      const R right = (ci == nx - 1 && !px) ? fb : FBxY[yi + 1];
+      return R(0.25) * (((-fa - up) + fb) + right);
+    };
+    const R inv_dx = R(g.inv_dx), inv_dy = R(g.inv_dy);
+    const int bx_lo = (STAGE == 3 && (i0 > 0 || px)) ? -1 : 0;   // halo face column for the epilogue
+    const int by_lo = (STAGE == 3 && (j0 > 0 || py)) ? -1 : 0;
+    for (int e = tid; e < G::NBX + G::NBY; e += NT) {
+      const bool isy = e >= G::NBX;
+      const int ee = isy ? e - G::NBX : e;
+      int li, lj;
+      if (!isy) { li = ee % G::BXW - 1; lj = ee / G::BXW; }
+      else { li = ee % G::BYW; lj = ee / G::BYW - 1; }
+      const int i = i0 + li, j = j0 + lj;
+      if ((!isy && li < bx_lo) || (isy && lj < by_lo)) continue;
+      if (i >= nx || j >= ny) continue;
+      const int gi = (i < 0) ? i + nx : i;
+      const int gj = (j < 0) ? j + ny : j;
+      const size_t idx = size_t(gj) * nx + gi;
+      R val;
+      if (!isy) {
+        const R e0 = Ez(i, j);
+        R dbx;
+        if (j > 0 || py) dbx = ((-e0) - (-Ez(i, j - 1))) * inv_dy;
+        else dbx = ((-Ez(i, 1)) - (-e0)) * inv_dy;           // outflow ylo: copy row 2
+        val = in[4][idx] + dt * dbx;
+        if (STAGE == 2) val = R(0.75) * u0[4][idx] + R(0.25) * val;
+        if (STAGE == 3) val = R(1.0 / 3.0) * u0[4][idx] + R(2.0 / 3.0) * val;
+        sBx[lj * G::BXW + (li + 1)] = val;
+      } else {
+        const R e0 = Ez(i, j);
+        R dby;
+        if (i > 0 || px) dby = -(((-e0) - (-Ez(i - 1, j))) * inv_dx);
+        else dby = -(((-Ez(1, j)) - (-e0)) * inv_dx);        // outflow xlo: copy column 2
+        val = in[5][idx] + dt * dby;
+        if (STAGE == 2) val = R(0.75) * u0[5][idx] + R(0.25) * val;
+        if (STAGE == 3) val = R(1.0 / 3.0) * u0[5][idx] + R(2.0 / 3.0) * val;
+        sBy[(lj + 1) * G::BYW + li] = val;
+      }
+    }
+    __syncthreads();
+
+    // ---- phase 3b: cell update -------------------------------------------------
+    double e_speed = 0.0, e_dmax = 0.0, e_dsum = 0.0, e_bmax = 0.0, e_mass = 0.0, e_en = 0.0;
+    unsigned floor_hits = 0;
+    const R ax = dt * R(g.dy);   // x-face weight (dt*dx in the square reference)
+    const R ay = dt * R(g.dx);
+    for (int c = tid; c < TX * TY; c += NT) {
+      const int li = c % TX, lj = c / TX;
+      const int i = i0 + li, j = j0 + lj;
+      if (i >= nx || j >= ny) continue;
+      const size_t idx = size_t(j) * nx + i;
+      const int fxr = (lj + 1) * G::FXW + (li + 1);  // x face i+1/2
+      const int fyt = (lj + 1) * G::FYW + (li + 1);  // y face j+1/2
+      R U[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        // update_conserved (src/mhd_flux.f90:20-76): x pass, then y pass
+        R F = in[q][idx];
+        const R* fx = sFx + q * G::NFX;
+        const R* fy = sFy + q * G::NFY;
+        if (i > 0 || px) F = (F - ax * fx[fxr]) + ax * fx[fxr - 1];
+        else F = F - ax * fx[fxr];
+        if (j > 0 || py) F = (F - ay * fy[fyt]) + ay * fy[fyt - G::FYW];
+        else F = F - ay * fy[fyt];
+        U[q] = F;
+      }
+      const int pc = (lj + 2) * G::PX + (li + 2);
+      const R cr = sP[0 * G::NP + pc], cu = sP[1 * G::NP + pc], cv = sP[2 * G::NP + pc];
+      const R cP = sP[3 * G::NP + pc], cBx = sP[4 * G::NP + pc], cBy = sP[5 * G::NP + pc];
+      // apply_conserved_floors with the stage's (pre-CT) cell B (src/main.f90:113)
+      floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
+      // outflow boundary flux correction (src/main.f90:118-148)
+      if (!px && i == 0) {
+        const R hb = R(0.5) * (cBx * cBx + cBy * cBy);
+        const R en = ((cP - hb) / (gamma - R(1)) + R(0.5) * cr * (cu * cu + cv * cv)) + hb;
+        U[0] = U[0] + ax * cr * cu;
+        U[1] = U[1] + ax * ((cr * (cu * cu) + cP) - cBx * cBx);
+        U[2] = U[2] + ax * (cr * cu * cv - cBx * cBy);
+        U[3] = U[3] + ax * ((en + cP) * cu - cBx * (cBx * cu + cBy * cv));
+      }
+      if (!py && j == 0) {
+        const R hb = R(0.5) * (cBx * cBx + cBy * cBy);
+        const R en = ((cP - hb) / (gamma - R(1)) + R(0.5) * cr * (cu * cu + cv * cv)) + hb;
+        U[0] = U[0] + ay * cr * cv;
+        U[2] = U[2] + ay * ((cr * (cv * cv) + cP) - cBy * cBy);
+        U[1] = U[1] + ay * (cr * cv * cu - cBy * cBx);
+        U[3] = U[3] + ay * ((en + cP) * cv - cBy * (cBy * cv + cBx * cu));
+      }
+      // RK blend + floors with the same stale cell B (src/main.f90:202-208, 261-267)
+      if (STAGE == 2) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) U[q] = R(0.75) * u0[q][idx] + R(0.25) * U[q];
+      }
+      if (STAGE == 3) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) U[q] = R(1.0 / 3.0) * u0[q][idx] + R(2.0 / 3.0) * U[q];
+      }
+      if (STAGE >= 2) floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
+      const R bxn = sBx[lj * G::BXW + (li + 1)];
+      const R byn = sBy[(lj + 1) * G::BYW + li];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) out[q][idx] = U[q];
+      out[4][idx] = bxn;
+      out[5][idx] = byn;
+
+      if (STAGE == 3) {
+        // epilogue: primitives of U^{n+1} (next step's CFL, src/main.f90:69-79),
+        // div B (src/main.f90:276), |B| and totals.
+        const R bxm = sBx[lj * G::BXW + li];
+        const R bym = sBy[lj * G::BYW + li];
+        const bool hx = (i > 0) || px, hy = (j > 0) || py;
+        const double Bx = hx ? 0.5 * (double(bxn) + double(bxm)) : double(bxn);
+        const double By = hy ? 0.5 * (double(byn) + double(bym)) : double(byn);
+        Prim<double> pr = get_primitive<double>(double(U[0]), double(U[1]), double(U[2]), double(U[3]),
+                                                Bx, By, g.gamma, g.vol);
+        e_speed = fmax(e_speed, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+        const double d = fabs(divb_cell(double(bxn), double(bxm), double(byn), double(bym), hx, hy,
+                                        g.inv_dx, g.inv_dy, g.square != 0));
+        e_dmax = fmax(e_dmax, d);
+        e_dsum += d;
+        e_bmax = fmax(e_bmax, sqrt(Bx * Bx + By * By));
+        e_mass += double(U[0]);
+        e_en += double(U[3]);
+      }
+    }
+    if (a.counters) {
+      unsigned s = __reduce_add_sync(0xffffffffu, floor_hits);
+      if ((tid & 31) == 0 && s) atomicAdd(&ctl->floor_hits, (unsigned long long)s);
+    }
+
+    if (STAGE == 3) {
+      const double r0 = block_reduce_max<NT>(e_speed, red);
+      const double r1 = block_reduce_max<NT>(e_dmax, red);
+      const double r2 = block_reduce_sum<NT>(e_dsum, red);
+      const double r3 = block_reduce_max<NT>(e_bmax, red);
+      const double r4 = block_reduce_sum<NT>(e_mass, red);
+      const double r5 = block_reduce_sum<NT>(e_en, red);
+      if (tid == 0) {
+        double* p = a.partials + size_t(w) * NPART;
+        p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = r5;
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
+        s_last = (prev == unsigned(g.tiles_x * g.tiles_y - 1)) ? 1 : 0;
+      }
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        member_finish<NT>(g, ctl, a.partials, g.tiles_x * g.tiles_y, true, red);
+      }
+    }
+    __syncthreads();  // shared memory is reused by the next tile
+  }
+}
+
+// ----------------------------------------------------------------------------
+// CFL kernel: dt of the current state (src/main.f90:69-83) without advancing
+// time; used before the first step after the state is set.
+// ----------------------------------------------------------------------------
+template <typename R, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
+  __shared__ double red[NT / 32];
+  __shared__ int s_last;
+  for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
+    const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
+    const Member& g = a.members[m];
+    Control* ctl = a.ctl + m;
+    const int nx = g.nx, ny = g.ny;
+    const int lt = w - g.tile_begin;
+    const int i0 = (lt % g.tiles_x) * TX;
+    const int j0 = (lt / g.tiles_x) * TY;
+    const R* in[6];
+    for (int q = 0; q < 6; ++q) in[q] = reinterpret_cast<const R*>(g.buf[ctl->parity][q]);
+    double sp = 0.0, dmx = 0.0, dsum = 0.0, bmx = 0.0, ms = 0.0, es = 0.0;
+    for (int c = threadIdx.x; c < TX * TY; c += NT) {
+      const int i = i0 + c % TX, j = j0 + c / TX;
+      if (i >= nx || j >= ny) continue;
+      const size_t k = size_t(j) * nx + i;
+      const double bxc = double(in[4][k]), byc = double(in[5][k]);
+      const bool hx = (i > 0) || g.periodic_x, hy = (j > 0) || g.periodic_y;
+      const double bxm = hx ? double(in[4][(i > 0) ? k - 1 : k + (nx - 1)]) : bxc;
+      const double bym = hy ? double(in[5][(j > 0) ? k - nx : k + size_t(ny - 1) * nx]) : byc;
+      const double Bx = hx ? 0.5 * (bxc + bxm) : bxc;
+      const double By = hy ? 0.5 * (byc + bym) : byc;
+      Prim<double> pr = get_primitive<double>(double(in[0][k]), double(in[1][k]), double(in[2][k]),
+                                              double(in[3][k]), Bx, By, g.gamma, g.vol);
+      sp = fmax(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+      const double d = fabs(divb_cell(bxc, bxm, byc, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
+      dmx = fmax(dmx, d);
+      dsum += d;
+      bmx = fmax(bmx, sqrt(Bx * Bx + By * By));
+      ms += double(in[0][k]);
+      es += double(in[3][k]);
+    }
+    const double r0 = block_reduce_max<NT>(sp, red);
+    const double r1 = block_reduce_max<NT>(dmx, red);
+    const double r2 = block_reduce_sum<NT>(dsum, red);
+    const double r3 = block_reduce_max<NT>(bmx, red);
+    const double r4 = block_reduce_sum<NT>(ms, red);
+    const double r5 = block_reduce_sum<NT>(es, red);
+    if (threadIdx.x == 0) {
+      double* p = a.partials + size_t(w) * NPART;
+      p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = r5;
+      __threadfence();
+      const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
+      s_last = (prev == unsigned(g.tiles_x * g.tiles_y - 1)) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      member_finish<NT>(g, ctl, a.partials, g.tiles_x * g.tiles_y, false, red);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace chimera

@@ -1,0 +1,181 @@
+/*
+ * chimera_gpu.h -- C-ABI of the B200 (sm_100a) drop-in for CHIMERA's per-step
+ * hot path: one SSP-RK3 step of the 2-D ideal-MHD finite-volume solver.
+ *
+ * The reference has no C-ABI: the path is the body of the Fortran time loop
+ * (src/main.f90:65-303) calling module subroutines on whole arrays.  Each entry
+ * point below names the reference code it replaces.  Plain C types only: a
+ * Fortran iso_c_binding interface, ctypes, or C/C++ can bind it directly.
+ *
+ * Arrays: real(8) (ld, ny) column-major with x fastest -- the Fortran layout of
+ * Mass, Momx, Momy, Energy (cell centred, multiplied by the cell volume) and the
+ * staggered face fields b_x (x face i+1/2) and b_y (y face j+1/2)
+ * (src/mhd_init.f90:44-47).  ld >= nx is the leading dimension in elements.
+ *
+ * Errors: every call returns CHIMERA_OK (0) or a negative CHIMERA_ERR_*.
+ * Nothing on this path prints, exits, traps or aborts.
+ * Threading: a handle owns one CUDA stream and is not thread safe; distinct
+ * handles are independent.  Calls are asynchronous on the handle's stream
+ * except *_get_state, *_diag and chimera_advance, which synchronise it.
+ */
+#ifndef CHIMERA_GPU_H
+#define CHIMERA_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Switch values are the reference's code numbering (src/mhd_config.f90:27-43). */
+#define CHIMERA_RIEMANN_RUSANOV 1
+#define CHIMERA_RIEMANN_HLLE 2
+#define CHIMERA_RIEMANN_HLLD 3
+#define CHIMERA_LIMITER_VAN_LEER 1
+#define CHIMERA_LIMITER_MC 2
+#define CHIMERA_BC_PERIODIC 1
+#define CHIMERA_BC_FIXED 2    /* behaves as outflow on this path (src/main.f90:349-354) */
+#define CHIMERA_BC_OUTFLOW 3
+#define CHIMERA_BC_INFLOW 4   /* behaves as outflow on this path */
+
+#define CHIMERA_FP64 0        /* plain FP64, bit-compatible with the reference expressions */
+#define CHIMERA_FP32_BULK 1   /* FP32 storage/arithmetic, FP64 pressure recovery, dt and sums */
+
+#define CHIMERA_HOST 0        /* pointer arguments are host memory */
+#define CHIMERA_DEVICE 1      /* pointer arguments are device memory */
+
+#define CHIMERA_OK 0
+#define CHIMERA_ERR_BAD_ARG -1       /* invalid argument (dims, switches, null pointer, ld) */
+#define CHIMERA_ERR_CUDA -2          /* a CUDA runtime call failed */
+#define CHIMERA_ERR_NONFINITE -3     /* the device status word reports a non-finite state */
+#define CHIMERA_ERR_TIMEOUT -4       /* a bounded device wait gave up */
+#define CHIMERA_ERR_UNSUPPORTED -5   /* valid in the reference but not on this path */
+#define CHIMERA_ERR_NO_DEVICE -6     /* no usable sm_100 device */
+#define CHIMERA_ERR_NOMEM -7         /* device allocation failed */
+#define CHIMERA_ERR_TOO_LARGE -8     /* size exceeds a fixed capacity */
+
+/* Build-time switches of src/mhd_config.f90:16-62, passed through so the
+ * Fortran program's own parameters are honoured. */
+typedef struct chimera_cfg {
+  int nx, ny;              /* N, N in the reference (nx == ny there) */
+  double dx, dy;           /* dx = boxsize/N (src/main.f90:34); dy == dx in the reference */
+  double gamma;
+  double courant;          /* courant_fac (0.3) */
+  double t_out;            /* tOut (0.01): dt is clipped to the next output time */
+  double t_end;            /* tEnd: steps stop once t >= t_end */
+  int bc_xlo, bc_xhi, bc_ylo, bc_yhi;   /* BC_xlo.. (src/mhd_config.f90:48-49) */
+  int riemann;             /* riemann_solver */
+  int limiter;             /* slope_limiter */
+  int use_slope_limiting;  /* useSlopeLimiting */
+  int mood;                /* fallback_2_MOOD */
+  int precision;           /* CHIMERA_FP64 or CHIMERA_FP32_BULK */
+} chimera_cfg;
+
+typedef struct chimera_diag_out {
+  double t;                /* simulation time after the last step */
+  double dt;               /* time step the next step will use (CFL + tOut clip) */
+  int output_count;        /* outputCount of src/main.f90:62,291 */
+  int active;              /* t < t_end */
+  unsigned long long steps;
+  double divb_max;         /* max |divB| over cells (compute_divB, src/mhd_field_ops.f90:60-117) */
+  double divb_mean;        /* sum |divB| / (nx ny), the reference's printed monitor (src/main.f90:299) */
+  double bmax;             /* max |B| of the cell-centred field */
+  double divb_rel;         /* max|divB| * min(dx,dy) / max|B| */
+  double mass;             /* sum of Mass (FP64) */
+  double energy;           /* sum of Energy (FP64) */
+  double cfl_speed;        /* max(c_f + |v|) */
+  unsigned long long mood_resets;  /* faces with a MOOD reset (if counters on) */
+  unsigned long long floor_hits;   /* cells with a conserved floor hit (if counters on) */
+  unsigned status;         /* device status word (0 = clean) */
+} chimera_diag_out;
+
+typedef struct chimera_handle chimera_handle;
+
+/* ---- single grid --------------------------------------------------------- */
+
+/* Create a solver for one grid.  stream: a cudaStream_t, or NULL to create one.
+ * Replaces the allocations of src/mhd_init.f90:99-164 for the path's arrays. */
+int chimera_create(const chimera_cfg* cfg, void* stream, chimera_handle** out);
+
+/* Copy a conserved state in (host or device arrays); marks dt stale.
+ * Replaces the module globals Mass..b_y (src/mhd_init.f90:44-47). */
+int chimera_set_state(chimera_handle* h, const double* Mass, const double* Momx,
+                      const double* Momy, const double* Energy, const double* b_x,
+                      const double* b_y, int ld, int where);
+
+/* Copy the conserved state out (synchronises).  Returns CHIMERA_ERR_NONFINITE
+ * if the device status word is set (the arrays are still copied). */
+int chimera_get_state(chimera_handle* h, double* Mass, double* Momx, double* Momy,
+                      double* Energy, double* b_x, double* b_y, int ld, int where);
+
+/* Set t and outputCount (src/main.f90:61-62); marks dt stale. */
+int chimera_set_time(chimera_handle* h, double t, int output_count);
+
+/* Advance nsteps SSP-RK3 steps: the loop body of src/main.f90:65-303 (CFL dt,
+ * tOut clip, three stages, t += dt, div B monitor, outputCount).  Steps stop
+ * early, on the device, once t >= t_end. */
+int chimera_step(chimera_handle* h, int nsteps);
+
+/* Run until t >= t_end or max_steps steps (do while (t < tEnd),
+ * src/main.f90:65); *steps_taken receives the count.  Synchronises. */
+int chimera_advance(chimera_handle* h, int max_steps, int* steps_taken);
+
+/* One RK stage k (1..3) with a given dt on the handle's stage buffers
+ * (src/main.f90:107-149, 155-208, 214-267): stage 1 reads U^n, writes U1;
+ * stage 2 reads U1 and U^n, writes U2; stage 3 reads U2 and U^n, writes U^n.
+ * For stage-level parity tests. */
+int chimera_stage(chimera_handle* h, int k, double dt);
+
+/* Read stage buffer b (0 = U^n, 1 = U1, 2 = U2), synchronising. */
+int chimera_get_stage_buffer(chimera_handle* h, int b, double* Mass, double* Momx,
+                             double* Momy, double* Energy, double* b_x, double* b_y,
+                             int ld, int where);
+
+/* Diagnostics of the last step or CFL evaluation (synchronises). */
+int chimera_diag(chimera_handle* h, chimera_diag_out* out);
+
+/* Count MOOD resets and floor hits on the device (off by default). */
+int chimera_set_counters(chimera_handle* h, int on);
+
+/* Time every kernel launch of the eager (non-graph) path with CUDA events on
+ * the handle's stream (no counterpart in the reference, which has no timers). */
+int chimera_set_profiling(chimera_handle* h, int on);
+
+/* Accumulated device time in ms and launch counts of [CFL, stage 1, stage 2,
+ * stage 3] since the last reset (synchronises). */
+int chimera_get_profile(chimera_handle* h, double* ms, long long* launches, int reset);
+
+/* The handle's stream (a cudaStream_t). */
+void* chimera_stream(chimera_handle* h);
+
+void chimera_destroy(chimera_handle* h);
+
+/* ---- batched ensembles (one persistent launch per stage over all members) -- */
+
+/* A batch of independent grids of uneven sizes.  All members share riemann,
+ * limiter, use_slope_limiting, mood and precision; sizes, spacing, gamma and
+ * boundary conditions are per member.  Replaces the sequential ensemble loop
+ * of scripts/run_mhd_MC.py:62-73. */
+int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream,
+                         chimera_handle** out);
+int chimera_batch_set_state(chimera_handle* h, int member, const double* Mass,
+                            const double* Momx, const double* Momy, const double* Energy,
+                            const double* b_x, const double* b_y, int ld, int where);
+int chimera_batch_get_state(chimera_handle* h, int member, double* Mass, double* Momx,
+                            double* Momy, double* Energy, double* b_x, double* b_y, int ld,
+                            int where);
+int chimera_batch_set_time(chimera_handle* h, int member, double t, int output_count);
+int chimera_batch_diag(chimera_handle* h, int member, chimera_diag_out* out);
+int chimera_batch_size(chimera_handle* h);
+
+/* Capture nsteps steps into a CUDA graph once and replay it on every
+ * chimera_step(h, nsteps) call with the same count (0 disables). */
+int chimera_set_graph_steps(chimera_handle* h, int nsteps);
+
+/* ---- misc ------------------------------------------------------------------ */
+const char* chimera_strerror(int code);
+int chimera_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHIMERA_GPU_H */

@@ -1,0 +1,74 @@
+"""The C-ABI library loads on a machine without a GPU and exports every entry
+point that include/chimera_gpu.h declares; argument validation needs no device."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "chimera_gpu.h")
+
+
+def declared_symbols(path):
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(chimera_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from chimera_b200 import build, gpu
+    if not os.path.exists(gpu.LIB_PATH):
+        build.build()
+    return gpu.lib()
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols(HEADER)
+    for s in ("chimera_create", "chimera_step", "chimera_set_state", "chimera_get_state",
+              "chimera_diag", "chimera_destroy", "chimera_batch_create", "chimera_strerror"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [s for s in declared_symbols(HEADER) if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_strerror(lib):
+    assert lib.chimera_strerror(0) == b"ok"
+    assert b"invalid" in lib.chimera_strerror(-1)
+    assert lib.chimera_strerror(12345) == b"unknown error"
+
+
+def _cfg(**kw):
+    from chimera_b200 import gpu
+    from chimera_b200.config import SolverConfig
+    base = dict(nx=16, ny=16, dx=1 / 16, dy=1 / 16, gamma=5 / 3)
+    base.update(kw)
+    return gpu.to_ccfg(SolverConfig(**base))
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(nx=3), -1),                  # N >= 4 (src/mhd_init.f90:208)
+    (dict(dx=0.0), -1),
+    (dict(gamma=1.0), -1),
+    (dict(riemann=4), -1),
+    (dict(limiter=0), -1),
+    (dict(bc=(1, 3, 1, 1)), -5),       # one-sided periodic: unsupported
+    (dict(bc=(1, 1, 5, 5)), -1),
+])
+def test_create_rejects_bad_config(lib, kw, code):
+    h = C.c_void_p()
+    cfg = _cfg(**kw)
+    assert lib.chimera_create(C.byref(cfg), None, C.byref(h)) == code
+    assert not h.value
+
+
+def test_null_arguments(lib):
+    h = C.c_void_p()
+    assert lib.chimera_create(None, None, C.byref(h)) == -1
+    assert lib.chimera_step(None, 1) == -1
+    assert lib.chimera_diag(None, None) == -1
+    lib.chimera_destroy(None)
