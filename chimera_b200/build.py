@@ -50,7 +50,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     hdr = _headers_digest()
-    objs = []
+    objs, jobs = [], []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         with open(src, "rb") as f:
@@ -60,12 +60,14 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             cmd = [nvcc] + ARCH + COMMON + flags + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0:
-                raise RuntimeError(f"nvcc failed for {unit}:\n{r.stderr}")
-            if ptxas_info:
-                sys.stderr.write(r.stderr)
+            jobs.append((unit, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         objs.append(obj)
+    for unit, proc in jobs:   # the units compile in parallel
+        _, err = proc.communicate()
+        if proc.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {unit}:\n{err}")
+        if ptxas_info:
+            sys.stderr.write(err)
     cmd = [nvcc] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs + ["-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -11,7 +11,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "../../include/chimera_gpu.h"
@@ -46,7 +49,11 @@ struct chimera_handle {
   bool own_stream = false;
   int device = 0;
   int num_sms = 148;
-  KernelSet ks{};
+  KernelSet ks{};                    // the active variant's kernels
+  std::vector<KernelSet> variants;
+  int cur_variant = 0;
+  int max_tiles = 0;                 // over all variants (partials / work-list capacity)
+  int dry = 0;
   int grid_stage[3] = {0, 0, 0};
   int grid_cfl = 0;
   int total_tiles = 0;
@@ -153,6 +160,7 @@ static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid) {
   a.slope_limiting = h->slope;
   a.mood = h->mood;
   a.counters = h->counters;
+  a.dry = h->dry;
   void* args[] = {&a};
   CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.nt), args, k.smem, h->stream));
   return CHIMERA_OK;
@@ -220,6 +228,55 @@ static int run_steps(chimera_handle* h, int nsteps) {
 
 static size_t cells_of(const chimera_cfg& c) { return size_t(c.nx) * size_t(c.ny); }
 
+static int tiles_for(const chimera_handle* h, int tx, int ty) {
+  int t = 0;
+  for (int m = 0; m < h->n; ++m) t += ((h->cfg[m].nx + tx - 1) / tx) * ((h->cfg[m].ny + ty - 1) / ty);
+  return t;
+}
+
+// Switch the tile decomposition to variant v: member tiling, work list and
+// persistent grid sizes (descriptors are re-uploaded; state is untouched).
+static int layout(chimera_handle* h, int v) {
+  h->ks = h->variants[v];
+  h->cur_variant = v;
+  const int tx = h->ks.stage[0][0].tx, ty = h->ks.stage[0][0].ty;
+  int tiles = 0;
+  for (int m = 0; m < h->n; ++m) {
+    Member& g = h->hm[m];
+    g.tiles_x = (g.nx + tx - 1) / tx;
+    g.tiles_y = (g.ny + ty - 1) / ty;
+    g.tile_begin = tiles;
+    tiles += g.tiles_x * g.tiles_y;
+  }
+  h->total_tiles = tiles;
+  std::vector<int> tm(tiles);
+  for (int m = 0; m < h->n; ++m)
+    for (int k = 0; k < h->hm[m].tiles_x * h->hm[m].tiles_y; ++k) tm[h->hm[m].tile_begin + k] = m;
+  CK(cudaMemcpyAsync(h->d_members, h->hm.data(), sizeof(Member) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_tile_member, tm.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int st = 0; st < 3; ++st) h->grid_stage[st] = grid_for(h, h->ks.stage[h->riemann - 1][st]);
+  h->grid_cfl = grid_for(h, h->ks.cfl);
+  drop_graph(h);
+  return CHIMERA_OK;
+}
+
+// Autotuner results per problem shape, shared by the handles of a process.
+using TuneKey = std::tuple<int, int, int, int, int, long long, int>;
+static std::map<TuneKey, int>& tune_cache() {
+  static std::map<TuneKey, int> c;
+  return c;
+}
+static std::mutex& tune_mutex() {
+  static std::mutex m;
+  return m;
+}
+static TuneKey tune_key(const chimera_handle* h) {
+  long long cells = 0;
+  for (int m = 0; m < h->n; ++m) cells += (long long)cells_of(h->cfg[m]);
+  return TuneKey(h->precision, h->riemann, h->limiter, h->mood, h->slope, cells, h->n);
+}
+
 extern "C" {
 
 int chimera_version(void) { return 10000; }
@@ -264,13 +321,18 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
   h->precision = cfgs[0].precision;
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  if (h->precision == CHIMERA_FP64) fp64_kernels(0, &h->ks);
-  else fp32_kernels(0, &h->ks);
-  for (int r = 0; r < 3; ++r)
-    for (int s = 0; s < 3; ++s)
-      cudaFuncSetAttribute(h->ks.stage[r][s].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           int(h->ks.stage[r][s].smem));
+  const int nv = (h->precision == CHIMERA_FP64) ? fp64_variant_count() : fp32_variant_count();
+  h->variants.resize(nv);
+  for (int v = 0; v < nv; ++v) {
+    if (h->precision == CHIMERA_FP64) fp64_kernels(v, &h->variants[v]);
+    else fp32_kernels(v, &h->variants[v]);
+    for (int r = 0; r < 3; ++r)
+      for (int st = 0; st < 3; ++st)
+        cudaFuncSetAttribute(h->variants[v].stage[r][st].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(h->variants[v].stage[r][st].smem));
+  }
   cudaGetLastError();
+  h->ks = h->variants[0];
   if (stream) {
     h->stream = (cudaStream_t)stream;
   } else {
@@ -280,21 +342,19 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
     }
     h->own_stream = true;
   }
-  // members, work list
-  const int tx = h->ks.stage[0][0].tx, ty = h->ks.stage[0][0].ty;
+  // members (tiling is set by layout())
   const int eb = h->ks.elem_bytes;
   h->hm.resize(n_members);
   size_t pool_bytes = 0;
   int tiles = 0;
+  for (int v = 0; v < nv; ++v)
+    tiles = std::max(tiles, tiles_for(h, h->variants[v].stage[0][0].tx, h->variants[v].stage[0][0].ty));
+  h->max_tiles = tiles;
   for (int m = 0; m < n_members; ++m) {
     const chimera_cfg& c = cfgs[m];
     Member& g = h->hm[m];
     memset(&g, 0, sizeof(g));
     g.nx = c.nx; g.ny = c.ny;
-    g.tiles_x = (c.nx + tx - 1) / tx;
-    g.tiles_y = (c.ny + ty - 1) / ty;
-    g.tile_begin = tiles;
-    tiles += g.tiles_x * g.tiles_y;
     g.periodic_x = c.bc_xlo == CHIMERA_BC_PERIODIC;
     g.periodic_y = c.bc_ylo == CHIMERA_BC_PERIODIC;
     g.square = (c.dx == c.dy) ? 1 : 0;
@@ -312,7 +372,6 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
     h->max_cells = std::max(h->max_cells, n);
     pool_bytes += 18 * ((n * eb + 255) / 256) * 256;
   }
-  h->total_tiles = tiles;
   h->dt_valid.assign(n_members, false);
   if (cudaMalloc(&h->pool, pool_bytes) != cudaSuccess) { cudaGetLastError(); chimera_destroy(h); return CHIMERA_ERR_NOMEM; }
   cudaMemsetAsync(h->pool, 0, pool_bytes, h->stream);
@@ -322,9 +381,6 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
     for (int b = 0; b < 3; ++b)
       for (int q = 0; q < 6; ++q) { h->hm[m].buf[b][q] = p; p += fb; }
   }
-  std::vector<int> tm(tiles);
-  for (int m = 0; m < n_members; ++m)
-    for (int k = 0; k < h->hm[m].tiles_x * h->hm[m].tiles_y; ++k) tm[h->hm[m].tile_begin + k] = m;
   std::vector<Control> ctl(n_members);
   for (int m = 0; m < n_members; ++m) {
     memset(&ctl[m], 0, sizeof(Control));
@@ -334,8 +390,8 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
   }
   if (cudaMalloc(&h->d_members, sizeof(Member) * n_members) != cudaSuccess ||
       cudaMalloc(&h->d_ctl, sizeof(Control) * n_members) != cudaSuccess ||
-      cudaMalloc(&h->d_part, sizeof(double) * NPART * size_t(tiles)) != cudaSuccess ||
-      cudaMalloc(&h->d_tile_member, sizeof(int) * size_t(tiles)) != cudaSuccess) {
+      cudaMalloc(&h->d_part, sizeof(double) * NPART * size_t(h->max_tiles)) != cudaSuccess ||
+      cudaMalloc(&h->d_tile_member, sizeof(int) * size_t(h->max_tiles)) != cudaSuccess) {
     cudaGetLastError();
     chimera_destroy(h);
     return CHIMERA_ERR_NOMEM;
@@ -347,12 +403,15 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
       return CHIMERA_ERR_NOMEM;
     }
   }
-  cudaMemcpyAsync(h->d_members, h->hm.data(), sizeof(Member) * n_members, cudaMemcpyHostToDevice, h->stream);
   cudaMemcpyAsync(h->d_ctl, ctl.data(), sizeof(Control) * n_members, cudaMemcpyHostToDevice, h->stream);
-  cudaMemcpyAsync(h->d_tile_member, tm.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, h->stream);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) { cudaGetLastError(); chimera_destroy(h); return CHIMERA_ERR_CUDA; }
-  for (int s = 0; s < 3; ++s) h->grid_stage[s] = grid_for(h, h->ks.stage[h->riemann - 1][s]);
-  h->grid_cfl = grid_for(h, h->ks.cfl);
+  int v0 = 0;
+  {
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    auto it = tune_cache().find(tune_key(h));
+    if (it != tune_cache().end()) v0 = it->second;
+  }
+  if (layout(h, v0) != CHIMERA_OK) { chimera_destroy(h); return CHIMERA_ERR_CUDA; }
   *out = h;
   return CHIMERA_OK;
 }
@@ -604,6 +663,69 @@ int chimera_get_profile(chimera_handle* h, double* ms, long long* launches, int 
     launches[k] = h->prof_n[k];
     if (reset) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
   }
+  return CHIMERA_OK;
+}
+
+int chimera_variant_count(chimera_handle* h) { return h ? int(h->variants.size()) : CHIMERA_ERR_BAD_ARG; }
+
+int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_y, int* threads) {
+  if (!h) return CHIMERA_ERR_BAD_ARG;
+  if (variant) *variant = h->cur_variant;
+  if (tile_x) *tile_x = h->ks.stage[0][0].tx;
+  if (tile_y) *tile_y = h->ks.stage[0][0].ty;
+  if (threads) *threads = h->ks.stage[0][0].nt;
+  return CHIMERA_OK;
+}
+
+int chimera_set_variant(chimera_handle* h, int v) {
+  if (!h || v < 0 || v >= int(h->variants.size())) return CHIMERA_ERR_BAD_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return layout(h, v);
+}
+
+int chimera_autotune(chimera_handle* h, int reps, int* chosen, double* best_ms) {
+  if (!h || reps < 1) return CHIMERA_ERR_BAD_ARG;
+  int rc = ensure_dt(h);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int saved_prof = h->profiling;
+  h->profiling = 0;
+  int best = h->cur_variant;
+  float best_t = 1e30f;
+  for (int v = 0; v < int(h->variants.size()) && rc == CHIMERA_OK; ++v) {
+    rc = layout(h, v);
+    if (rc) break;
+    h->dry = 1;
+    rc = one_step(h);                       // warm-up
+    if (rc == CHIMERA_OK) {
+      cudaEventRecord(e0, h->stream);
+      for (int r = 0; r < reps && rc == CHIMERA_OK; ++r) rc = one_step(h);
+      cudaEventRecord(e1, h->stream);
+    }
+    h->dry = 0;
+    float ms = 0.f;
+    if (rc == CHIMERA_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+      if (ms < best_t) { best_t = ms; best = v; }
+    } else if (rc == CHIMERA_OK) {
+      rc = CHIMERA_ERR_CUDA;
+    }
+  }
+  h->dry = 0;
+  h->profiling = saved_prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  int lrc = layout(h, best);
+  if (rc) return rc;
+  if (lrc) return lrc;
+  {
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    tune_cache()[tune_key(h)] = best;
+  }
+  if (chosen) *chosen = best;
+  if (best_ms) *best_ms = double(best_t) / reps;
   return CHIMERA_OK;
 }
 

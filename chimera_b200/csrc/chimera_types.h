@@ -53,6 +53,7 @@ struct StageArgs {
   int total_tiles;
   int limiter, slope_limiting, mood;
   int counters;            // count MOOD resets / floor hits
+  int dry;                 // timing run: write scratch only, leave Control untouched
 };
 
 }  // namespace chimera

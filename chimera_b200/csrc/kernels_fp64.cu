@@ -7,12 +7,12 @@
 namespace chimera {
 
 namespace {
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, int MINB>
 void fill(KernelSet* ks) {
   using G = TileGeom<TX, TY>;
   const size_t smem = G::template smem_bytes<double>();
 #define CHIMERA_ENTRY(S, K) \
-  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel<double, S, K, TX, TY, NT>, smem, TX, TY, NT}
+  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel<double, S, K, TX, TY, NT, MINB>, smem, TX, TY, NT}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
@@ -22,11 +22,16 @@ void fill(KernelSet* ks) {
 }
 }  // namespace
 
-int fp64_variant_count() { return 1; }
+// Tile shapes and occupancy targets the autotuner chooses from.
+int fp64_variant_count() { return 5; }
 
 void fp64_kernels(int variant, KernelSet* out) {
   switch (variant) {
-    default: fill<32, 16, 256>(out); break;
+    case 1: fill<32, 16, 256, 2>(out); break;
+    case 2: fill<32, 8, 128, 4>(out); break;
+    case 3: fill<64, 8, 256, 2>(out); break;
+    case 4: fill<16, 16, 128, 4>(out); break;
+    default: fill<32, 16, 256, 1>(out); break;
   }
 }
 

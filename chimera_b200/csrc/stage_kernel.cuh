@@ -169,8 +169,8 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
 //            the parity.  (Writing U^{n+1} over U^n in place would race: the
 //            epilogue's halo faces read U^n at the neighbour tile's cells.)
 // ----------------------------------------------------------------------------
-template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) stage_kernel(StageArgs a) {
+template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   using G = TileGeom<TX, TY>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a) {
       const R inv_h = R(ydir ? g.inv_dy : g.inv_dx);
       const R inv_2h = R(ydir ? g.inv_2dy : g.inv_2dx);
       const R hh = R(ydir ? g.hy : g.hx);             // 0.5 * spacing
-      R L[6], Rv[6], C0[6];
+      R L[6], Rv[6];
       bool reset = false;
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
@@ -289,17 +289,17 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a) {
           vL = dmax(vL, R(1.0e-8));
           vR = dmax(vR, R(1.0e-8));
         }
-        L[q] = vL; Rv[q] = vR; C0[q] = f0;
+        L[q] = vL; Rv[q] = vR;
       }
       // thermal_pressure_check (src/mhd_derivatives.f90:232-293): reset all six
       // fields of a face slot to the low cell's values.
       if (L[3] - R(0.5) * (L[4] * L[4] + L[5] * L[5]) < K<R>::P_floor) {
 #pragma unroll
-        for (int q = 0; q < 6; ++q) L[q] = C0[q];
+        for (int q = 0; q < 6; ++q) L[q] = sP[q * G::NP + pa];
       }
       if (Rv[3] - R(0.5) * (Rv[4] * Rv[4] + Rv[5] * Rv[5]) < K<R>::P_floor) {
 #pragma unroll
-        for (int q = 0; q < 6; ++q) Rv[q] = C0[q];
+        for (int q = 0; q < 6; ++q) Rv[q] = sP[q * G::NP + pa];
       }
       mood_resets += reset ? 1u : 0u;
       // compute_fluxes, rotated for y faces (src/main.f90:394-401)
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a) {
       dst[3 * NF + ff] = F.energy;
       dst[4 * NF + ff] = F.bt;                     // By flux (x faces) / Bx flux (y faces)
     }
-    if (a.counters) {
+    if (a.counters && !a.dry) {
       unsigned s = __reduce_add_sync(0xffffffffu, mood_resets);
       if ((tid & 31) == 0 && s) atomicAdd(&ctl->mood_resets, (unsigned long long)s);
     }
@@ -458,12 +458,12 @@ __global__ void __launch_bounds__(NT) stage_kernel(StageArgs a) {
         e_en += double(U[3]);
       }
     }
-    if (a.counters) {
+    if (a.counters && !a.dry) {
       unsigned s = __reduce_add_sync(0xffffffffu, floor_hits);
       if ((tid & 31) == 0 && s) atomicAdd(&ctl->floor_hits, (unsigned long long)s);
     }
 
-    if (STAGE == 3) {
+    if (STAGE == 3 && !a.dry) {
       const double r0 = block_reduce_max<NT>(e_speed, red);
       const double r1 = block_reduce_max<NT>(e_dmax, red);
       const double r2 = block_reduce_sum<NT>(e_dsum, red);

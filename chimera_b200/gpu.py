@@ -89,6 +89,11 @@ def lib():
         L.chimera_set_graph_steps.argtypes = [P, C.c_int]
         L.chimera_set_profiling.argtypes = [P, C.c_int]
         L.chimera_get_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int]
+        L.chimera_autotune.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.chimera_variant_count.argtypes = [P]
+        L.chimera_set_variant.argtypes = [P, C.c_int]
+        L.chimera_get_variant.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int)]
         L.chimera_stream.argtypes = [P]
         L.chimera_stream.restype = P
         _lib = L
@@ -230,3 +235,22 @@ class Solver:
         _check(lib().chimera_get_profile(self._h, ms, n, int(bool(reset))), "get_profile")
         names = ("cfl", "stage1", "stage2", "stage3")
         return {k: {"ms": ms[i], "launches": n[i]} for i, k in enumerate(names)}
+
+    def autotune(self, reps: int = 3):
+        """Time every tile variant on the current state; keep the fastest."""
+        v = C.c_int()
+        ms = C.c_double()
+        _check(lib().chimera_autotune(self._h, int(reps), C.byref(v), C.byref(ms)), "autotune")
+        return v.value, ms.value
+
+    def variant_count(self) -> int:
+        return lib().chimera_variant_count(self._h)
+
+    def set_variant(self, v: int):
+        _check(lib().chimera_set_variant(self._h, int(v)), "set_variant")
+
+    def variant(self):
+        v, tx, ty, nt = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib().chimera_get_variant(self._h, C.byref(v), C.byref(tx), C.byref(ty), C.byref(nt)),
+               "get_variant")
+        return {"variant": v.value, "tile": (tx.value, ty.value), "threads": nt.value}

@@ -170,6 +170,16 @@ int chimera_batch_size(chimera_handle* h);
  * chimera_step(h, nsteps) call with the same count (0 disables). */
 int chimera_set_graph_steps(chimera_handle* h, int nsteps);
 
+/* ---- tile-shape autotuner (no counterpart in the reference) --------------------
+ * Each precision is compiled in several tile shapes / occupancy targets.  The
+ * autotuner times reps dry RK3 steps of every variant on the handle's current
+ * state (scratch buffers only; the state and time-loop counters are untouched)
+ * and keeps the fastest; the choice is cached per problem shape for the process. */
+int chimera_autotune(chimera_handle* h, int reps, int* chosen, double* best_ms_per_step);
+int chimera_variant_count(chimera_handle* h);
+int chimera_set_variant(chimera_handle* h, int variant);
+int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_y, int* threads);
+
 /* ---- misc ------------------------------------------------------------------ */
 const char* chimera_strerror(int code);
 int chimera_version(void);

@@ -223,3 +223,41 @@ def test_rotor_1024_full_size(G, oracle):
     for q in range(6):
         assert np.array_equal(out[q], ref.a[q]), q
     assert s.diag()["divb_rel"] <= DIVB_TOL
+
+
+@pytest.mark.parametrize("solver", [RUSANOV, HLLE, HLLD])
+def test_every_tile_variant_bitwise(G, oracle, solver):
+    """Every compiled tile shape / occupancy variant gives the same bits."""
+    cfg, st = P.orszag_tang(70, riemann=solver)
+    cfg = cfg.replace(bc=(BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW))
+    ref = oracle.State(st)
+    oracle.run(cfg, ref, 8)
+    s = G.Solver(cfg)
+    for v in range(s.variant_count()):
+        s.set_state(st)
+        s.set_time(0.0, 1)
+        s.set_variant(v)
+        s.step(8)
+        out = s.get_state()
+        for q in range(6):
+            assert np.array_equal(out[q], ref.a[q]), (v, s.variant(), q)
+
+
+def test_autotune_keeps_state(G, oracle):
+    """Autotuning runs dry steps only: state and time-loop counters unchanged."""
+    cfg, st = P.rotor(128)
+    s = G.Solver(cfg)
+    s.set_state(st)
+    s.step(2)
+    before, d0 = s.get_state(), s.diag()
+    v, ms = s.autotune(reps=2)
+    assert 0 <= v < s.variant_count() and ms > 0
+    after, d1 = s.get_state(), s.diag()
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
+    assert (d0["t"], d0["steps"], d0["dt"]) == (d1["t"], d1["steps"], d1["dt"])
+    s.step(3)
+    ref = oracle.State(st)
+    oracle.run(cfg, ref, 5)
+    for x, y in zip(s.get_state(), ref.a):
+        assert np.array_equal(x, y)
