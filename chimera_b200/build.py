@@ -26,6 +26,7 @@ UNITS = {
     "kernels_fp64.cu": ["--fmad=false"],
     "kernels_fp32.cu": ["--fmad=true"],
     "chimera_api.cu": [],
+    "noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -180,6 +180,30 @@ int chimera_variant_count(chimera_handle* h);
 int chimera_set_variant(chimera_handle* h, int variant);
 int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_y, int* threads);
 
+/* ---- one step without device allocation ---------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc --
+ * a host code whose device memory is all owned by its own allocator, a time
+ * loop that must not pay cudaMalloc's implicit device synchronisation, or a
+ * program that forbids allocation after initialisation -- this advances a
+ * caller-owned FP64 state by one SSP-RK3 step (CFL dt with the tOut clip, the
+ * three stages, t += dt, outputCount) exactly as chimera_step does, without
+ * allocating anything: its stage buffers and reductions live in one fixed
+ * file-scope device array (about 6.5 MB) that every GPU which loads the
+ * library holds until the process exits.
+ *   - Mass..b_y: device pointers to dense (nx, ny) arrays, x fastest, updated
+ *     in place; cfg->precision must be CHIMERA_FP64.
+ *   - nx*ny above CHIMERA_NOALLOC_MAX_CELLS returns CHIMERA_ERR_TOO_LARGE.
+ *   - *t and *output_count are read and advanced; *dt_next (optional) receives
+ *     the dt the next step will take.  The call synchronises the stream.
+ *   - The first call on a device looks up the scratch's device address; make
+ *     that first call before any stream capture.
+ *   - Every call shares the one scratch array: calls that overlap on the GPU
+ *     (other host threads, other streams) race and must be serialised. */
+#define CHIMERA_NOALLOC_MAX_CELLS 65536
+int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, double* Momx, double* Momy,
+                             double* Energy, double* b_x, double* b_y, double* t,
+                             int* output_count, double* dt_next, void* stream);
+
 /* ---- misc ------------------------------------------------------------------ */
 const char* chimera_strerror(int code);
 int chimera_version(void);
