@@ -44,6 +44,15 @@ def parse():
     p.add_argument("--n", type=int, default=1024, help="grid size (default: the rotor workload)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--precision", choices=("fp64", "fp32"), default="fp64",
+                   help="precision form of the rotor measurement")
+    p.add_argument("--ensemble", choices=("on", "off", "only"), default="on",
+                   help="also measure the FP32-batched GRF ensemble against the FP64 form")
+    p.add_argument("--ens-scale", type=int, default=1,
+                   help="divide the ensemble member counts (1 = 256x128^2 + 192x256^2 + 64x512^2)")
+    p.add_argument("--ens-steps", type=int, default=200)
+    p.add_argument("--ens-variant", type=int, default=-1,
+                   help="force a tile variant for the ensemble (-1: autotune)")
     return p.parse_args()
 
 
@@ -193,12 +202,22 @@ def run_reference(args, world, rank):
 def run_chimera(args, world, rank, local):
     import torch
     from chimera_b200 import gpu, problems
+    from chimera_b200.config import FP32_BULK, FP64
 
     torch.cuda.set_device(local)
+    ens = None
+    if args.ensemble != "off":
+        ens = run_ensemble(args, world)
+        if args.ensemble == "only":
+            if rank == 0:
+                print(json.dumps({"ensemble": ens}), flush=True)
+            return
     n = args.n
     cells = n * n
     cfg, st = problems.rotor(n)
-    cfg = cfg.replace(t_end=1e30)     # keep stepping past t=0.15; per-step work is unchanged
+    prec = FP32_BULK if args.precision == "fp32" else FP64
+    esize = 4 if prec == FP32_BULK else 8
+    cfg = cfg.replace(t_end=1e30, precision=prec)   # keep stepping past t=0.15; per-step work is unchanged
     s = gpu.Solver(cfg)
     s.set_state(st)
     ext = torch.cuda.ExternalStream(s.stream)
@@ -237,10 +256,10 @@ def run_chimera(args, world, rank, local):
     avg = {k: v["ms"] / v["launches"] for k, v in prof.items() if v["launches"]}
     dom = max((k for k in avg if k.startswith("stage")), key=lambda k: avg[k])
     kidx = int(dom[-1])
-    alg_bytes = STAGE_ACCESSES[kidx] * 8 * cells
+    alg_bytes = STAGE_ACCESSES[kidx] * esize * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg[dom] * 1e-3) / 1e9
-    traffic = profile_traffic(f"fp64_hlle_{dom}_rotor{n}")
+    traffic = profile_traffic(f"{args.precision}_hlle_{dom}_rotor{n}")
 
     # --- end to end through the C-ABI with host buffers: every step copies the
     #     state in from pinned host memory, advances one step, copies it out.
@@ -282,14 +301,15 @@ def run_chimera(args, world, rank, local):
         line = {
             "metric": "zone-cycles/s", "value": value, "unit": "zone-cycles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec == FP32_BULK else "f64",
             "data": "synthetic (analytic rotor initial state)",
             "config": {"workload": WORKLOAD, "cells": cells, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (3 state sets x 48 MB > 126 MB)",
-                       "hbm_fraction": value / world * BYTES_PER_ZC_FP64 / (hbm * 1e9),
+                       "hbm_fraction": value / world * 48 * esize / (hbm * 1e9),
                        "tile": vinfo,
-                       "bytes_per_zone_cycle": BYTES_PER_ZC_FP64},
-            "roofline": {"bound": "hbm", "kernel": f"stage_kernel<double,HLLE,{kidx}>",
+                       "bytes_per_zone_cycle": 48 * esize},
+            "roofline": {"bound": "hbm", "kernel": f"stage kernel ({args.precision}, HLLE, stage {kidx})",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes,
@@ -298,9 +318,79 @@ def run_chimera(args, world, rank, local):
             "e2e": e2e,
             "gpu_launches": 3 * args.steps,
             "clocks": ck,
+            "forms": ens,
         }
         print(json.dumps(line), flush=True)
     s.close()
+
+
+def run_ensemble(args, world):
+    """The batched GRF ensemble (one persistent launch per stage over all
+    members of uneven sizes, CUDA-graph replay) in the FP32-bulk form and in the
+    plain FP64 form from the same seeded states.  The FP64 GPU form reproduces
+    the FP64 oracle bit for bit (tests/test_gpu_parity.py, test_gpu_batch.py),
+    so the FP32 form's L1 error is measured against it on the full ensemble."""
+    import numpy as np
+    import torch
+    from chimera_b200 import ensemble
+    from chimera_b200.config import FP32_BULK, FP64
+
+    steps = args.ens_steps
+    graph = 10 if steps % 10 == 0 else 1
+    res = {}
+    finals = {}
+    hbm, _ = peaks()
+    for name, prec in (("fp32_batched", FP32_BULK), ("fp64_batched", FP64)):
+        cfgs, states = ensemble.grf_ensemble(args.ens_scale, prec)
+        cells = ensemble.cells(cfgs)
+        s = ensemble.make_batch(cfgs, states)
+        s.step(1)
+        if args.ens_variant >= 0:
+            s.set_variant(args.ens_variant)
+        else:
+            s.autotune(reps=2)
+        # restart from the initial states so both forms take the same steps
+        for m, st in enumerate(states):
+            s.set_state(st, member=m)
+            s.set_time(0.0, 1, member=m)
+        s.set_graph_steps(graph)
+        ext = torch.cuda.ExternalStream(s.stream)
+        s.step(graph)                         # capture the graph (not timed)
+        for m, st in enumerate(states):
+            s.set_state(st, member=m)
+            s.set_time(0.0, 1, member=m)
+        s.step(0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        e0.record(ext)
+        for _ in range(steps // graph):
+            s.step(graph)
+        e1.record(ext)
+        e1.synchronize()
+        ms = dist_max(e0.elapsed_time(e1), world)
+        esize = 4 if prec == FP32_BULK else 8
+        zcs = world * cells * steps / (ms * 1e-3)
+        res[name] = {"value": zcs, "unit": "zone-cycles/s", "ms": ms, "steps": steps,
+                     "members": len(cfgs), "cells": cells, "tile": s.variant(),
+                     "bytes_per_zone_cycle": 48 * esize,
+                     "hbm_fraction": zcs / world * 48 * esize / (hbm * 1e9),
+                     "graph_steps": graph}
+        finals[name] = [s.get_state(member=m) for m in range(len(cfgs))]
+        s.close()
+    num = np.zeros(6)
+    den = np.zeros(6)
+    for a, b in zip(finals["fp32_batched"], finals["fp64_batched"]):
+        for q in range(6):
+            num[q] += np.sum(np.abs(a[q] - b[q]))
+            den[q] += np.sum(np.abs(b[q]))
+    l1 = (num / den).tolist()
+    res["fp32_l1_vs_fp64"] = dict(zip(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y"), l1))
+    res["fp32_over_fp64"] = res["fp32_batched"]["value"] / res["fp64_batched"]["value"]
+    res["workload"] = (f"GRF ensemble, {res['fp32_batched']['members']} members of uneven sizes "
+                       f"(128^2/256^2/512^2), periodic, Rusanov + MC + MOOD, {steps} RK3 steps")
+    return res
 
 
 def main():

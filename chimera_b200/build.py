@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC, "-I" + INCLUDE]
 UNITS = {
     "kernels_fp64.cu": ["--fmad=false"],
-    "kernels_fp32.cu": ["--fmad=true"],
+    "kernels_fp32.cu": ["-use_fast_math"],
     "chimera_api.cu": [],
     "noalloc.cu": ["--fmad=false"],
 }

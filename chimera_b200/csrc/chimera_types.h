@@ -28,6 +28,7 @@ struct Member {
   double inv_2dx, inv_2dy; // 1/(2 dx), 1/(2 dy)
   double hx, hy;           // 0.5*dx, 0.5*dy
   double gamma, vol, len;  // vol = dx*dy, len = min(dx, dy)
+  double inv_vol;          // 1/vol (FP32-bulk pressure recovery)
   double courant, t_out, t_end;
   void* buf[3][6];
   void* e64[3];            // FP32-bulk form: FP64 Energy per buffer (unused in FP64)

@@ -54,20 +54,22 @@ __device__ __forceinline__ Prim<R> get_primitive(R M, R Mx, R My, R E, R Bx, R B
   return p;
 }
 
-// FP32-bulk form: the storage / bulk type is float but the pressure recovery
-// p = (gamma-1)(E - rho v^2/2 - B^2/2) + B^2/2 is done in FP64 (the
-// cancellation at low plasma beta), then rounded to float.
-__device__ __forceinline__ Prim<float> get_primitive_mixed(float M, float Mx, float My, double E,
+// FP32-bulk form: storage and bulk arithmetic are FP32, but the pressure
+// recovery p = (gamma-1)(E/vol - rho v^2/2 - B^2/2) + B^2/2 -- a small
+// difference of large terms at low plasma beta -- is done in FP64 from the
+// FP32 inputs, then rounded to FP32.  Same floors as get_primitive.
+__device__ __forceinline__ Prim<float> get_primitive_mixed(float M, float Mx, float My, float E,
                                                            float Bx, float By, double gamma,
-                                                           double inv_vol) {
+                                                           double inv_vol, float inv_volf) {
   Prim<float> p;
-  float r = fmaxf(float(double(M) * inv_vol), 1.0e-12f);
-  float rv = float(double(r) / inv_vol);
-  float u = Mx / rv;
-  float v = My / rv;
-  double halfB2 = 0.5 * (double(Bx) * double(Bx) + double(By) * double(By));
-  double ke = 0.5 * double(r) * (double(u) * double(u) + double(v) * double(v));
-  double P = ((E * inv_vol - ke) - halfB2) * (gamma - 1.0) + halfB2;
+  const float r = fmaxf(M * inv_volf, 1.0e-12f);
+  const float ir = 1.0f / r;
+  const float u = (Mx * inv_volf) * ir;
+  const float v = (My * inv_volf) * ir;
+  const double rd = r, ud = u, vd = v, bx = Bx, by = By;
+  const double halfB2 = 0.5 * (bx * bx + by * by);
+  const double ke = 0.5 * rd * (ud * ud + vd * vd);
+  double P = ((double(E) * inv_vol - ke) - halfB2) * (gamma - 1.0) + halfB2;
   P = fmax(P, 1.0e-12);
   P = fmax(P, halfB2 + 1.0e-10 * (ke + halfB2));
   p.rho = r; p.vx = u; p.vy = v; p.P = float(P); p.Bx = Bx; p.By = By;

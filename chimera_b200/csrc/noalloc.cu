@@ -120,6 +120,7 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   g.gamma = cfg->gamma;
   g.vol = cfg->dx * cfg->dy;
   g.len = (cfg->dx < cfg->dy) ? cfg->dx : cfg->dy;
+  g.inv_vol = 1.0 / g.vol;
   g.courant = cfg->courant;
   g.t_out = cfg->t_out;
   g.t_end = cfg->t_end;

@@ -229,7 +229,12 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
       else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
       if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
       else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
-      Prim<R> pr = get_primitive<R>(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, gamma, vol);
+      Prim<R> pr;
+      if constexpr (sizeof(R) == 4)
+        pr = get_primitive_mixed(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, g.gamma,
+                                 g.inv_vol, float(g.inv_vol));
+      else
+        pr = get_primitive<R>(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, gamma, vol);
       sP[0 * G::NP + p] = pr.rho;
       sP[1 * G::NP + p] = pr.vx;
       sP[2 * G::NP + p] = pr.vy;
@@ -244,8 +249,9 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     for (int f = tid; f < G::NFX + G::NFY; f += NT) {
       const bool ydir = f >= G::NFX;
       const int ff = ydir ? f - G::NFX : f;
-      const int W = ydir ? G::FYW : G::FXW;
-      const int li = ff % W, lj = ff / W;
+      // constant divisors in each branch (a runtime divisor costs a full integer division)
+      const int li = ydir ? ff % G::FYW : ff % G::FXW;
+      const int lj = ydir ? ff / G::FYW : ff / G::FXW;
       const int pa = (lj + 1) * G::PX + (li + 1);    // cell on the low side of the face
       const int on = ydir ? G::PX : 1;               // offset along the face normal
       const R inv_h = R(ydir ? g.inv_dy : g.inv_dx);

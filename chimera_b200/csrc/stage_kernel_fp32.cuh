@@ -1,0 +1,356 @@
+// stage_kernel_fp32.cuh -- the FP32-bulk stage kernel.
+//
+// Same stage operator and tile structure as stage_kernel (stage_kernel.cuh),
+// with the freedom the FP32 form has (it is checked against the FP64 oracle in
+// L1, not bit for bit) spent on fewer instructions per cell:
+//   * phase 1.5 computes each cell's limited x and y slopes and MOOD bounds
+//     once into shared memory; the FP64 kernel recomputes them for each face
+//     that touches the cell (twice per direction);
+//   * the translation unit is compiled with fast FP32 division and square
+//     root (-use_fast_math), about 1 ulp instead of correctly rounded.
+// Kept in FP64: the pressure recovery p = (gamma-1)(E - rho v^2/2 - B^2/2)
+// (get_primitive_mixed), the CFL dt reduction and the tOut clip, and the
+// conserved-total sums.  The per-cell CFL speed is computed in FP32.
+#pragma once
+#include "stage_kernel.cuh"
+
+namespace chimera {
+
+template <int TX, int TY> struct TileGeom32 : TileGeom<TX, TY> {
+  using B = TileGeom<TX, TY>;
+  static constexpr int SX = TX + 2, SY = TY + 2, NS = SX * SY;   // cells [i0-1, i0+TX] x [j0-1, j0+TY]
+  static constexpr size_t smem_bytes() {
+    return sizeof(float) * (size_t(6) * B::NP + size_t(24) * NS + size_t(5) * B::NFX + size_t(5) * B::NFY +
+                            B::NBX + B::NBY);
+  }
+};
+
+template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
+  using G = TileGeom32<TX, TY>;
+  using R = float;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sP = reinterpret_cast<R*>(smem_raw);       // [6][NP]   primitives, tile + 2 halo
+  R* sS = sP + 6 * G::NP;                       // [12][NS]  slopes: field q, dir d at (2q+d)
+  R* sLo = sS + 12 * G::NS;                     // [6][NS]   MOOD lower bounds
+  R* sHi = sLo + 6 * G::NS;                     // [6][NS]   MOOD upper bounds
+  R* sFx = sHi + 6 * G::NS;                     // [5][NFX]
+  R* sFy = sFx + 5 * G::NFX;                    // [5][NFY]
+  R* sBx = sFy + 5 * G::NFY;
+  R* sBy = sBx + G::NBX;
+  __shared__ double red[NT / 32];
+  __shared__ int s_last;
+
+  const int tid = threadIdx.x;
+  const bool slope_on = a.slope_limiting != 0;
+  const bool mood_on = a.mood != 0;
+  const bool van_leer = a.limiter == LIMITER_VAN_LEER;
+
+  for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
+    const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
+    const Member& g = a.members[m];
+    Control* ctl = a.ctl + m;
+    if (ctl->active == 0) continue;
+    const int nx = g.nx, ny = g.ny;
+    const int px = g.periodic_x, py = g.periodic_y;
+    const int lt = w - g.tile_begin;
+    const int i0 = (lt % g.tiles_x) * TX;
+    const int j0 = (lt / g.tiles_x) * TY;
+    const R gamma = R(g.gamma);
+    const R vol = R(g.vol);
+    const R dt = R(ctl->dt);
+    const int sbuf = ctl->parity, obuf = 1 - sbuf;
+    const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
+    const int out_buf = (STAGE == 2) ? 2 : obuf;
+    const R* __restrict__ in[6];
+    const R* __restrict__ u0[6];
+    R* __restrict__ out[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
+      u0[q] = reinterpret_cast<const R*>(g.buf[sbuf][q]);
+      out[q] = reinterpret_cast<R*>(g.buf[out_buf][q]);
+    }
+
+    // ---- phase 1: primitives (FP64 pressure recovery) -------------------------
+    for (int p = tid; p < G::NP; p += NT) {
+      const int qx = p % G::PX, qy = p / G::PX;
+      const int si = map_index(i0 - 2 + qx, nx, px);
+      const int sj = map_index(j0 - 2 + qy, ny, py);
+      const size_t idx = size_t(sj) * nx + si;
+      const R bxc = in[4][idx];
+      const R byc = in[5][idx];
+      R Bx, By;
+      if (si > 0) Bx = R(0.5) * (bxc + in[4][idx - 1]);
+      else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
+      if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
+      else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
+      const Prim<R> pr = get_primitive_mixed(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By,
+                                             g.gamma, g.inv_vol, float(g.inv_vol));
+      sP[0 * G::NP + p] = pr.rho;
+      sP[1 * G::NP + p] = pr.vx;
+      sP[2 * G::NP + p] = pr.vy;
+      sP[3 * G::NP + p] = pr.P;
+      sP[4 * G::NP + p] = pr.Bx;
+      sP[5 * G::NP + p] = pr.By;
+    }
+    __syncthreads();
+
+    // ---- phase 1.5: per-cell slopes and MOOD bounds -----------------------------
+    // apply_slope_limiter (src/mhd_derivatives.f90:50-127) or compute_gradients
+    // (:15-47); bounds of the 5-point stencil with the rho/P floor (:190-211).
+    const R inv_dx = R(g.inv_dx), inv_dy = R(g.inv_dy);
+    const R inv_2dx = R(g.inv_2dx), inv_2dy = R(g.inv_2dy);
+    for (int c = tid; c < G::NS; c += NT) {
+      const int cx = c % G::SX, cy = c / G::SX;
+      const int pc = (cy + 1) * G::PX + (cx + 1);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const R* s = sP + q * G::NP;
+        const R f0 = s[pc], xm = s[pc - 1], xp = s[pc + 1], ym = s[pc - G::PX], yp = s[pc + G::PX];
+        R sx, sy;
+        if (slope_on) {
+          if (van_leer) {
+            sx = limit_slope<R, LIMITER_VAN_LEER>((f0 - xm) * inv_dx, (xp - f0) * inv_dx);
+            sy = limit_slope<R, LIMITER_VAN_LEER>((f0 - ym) * inv_dy, (yp - f0) * inv_dy);
+          } else {
+            sx = limit_slope<R, LIMITER_MC>((f0 - xm) * inv_dx, (xp - f0) * inv_dx);
+            sy = limit_slope<R, LIMITER_MC>((f0 - ym) * inv_dy, (yp - f0) * inv_dy);
+          }
+        } else {
+          sx = (xp - xm) * inv_2dx;
+          sy = (yp - ym) * inv_2dy;
+        }
+        sS[(2 * q + 0) * G::NS + c] = sx;
+        sS[(2 * q + 1) * G::NS + c] = sy;
+        if (mood_on) {
+          R lo = fminf(fminf(fminf(fminf(f0, xp), xm), yp), ym);
+          const R hi = fmaxf(fmaxf(fmaxf(fmaxf(f0, xp), xm), yp), ym);
+          if (q == 0 || q == 3) lo = fmaxf(R(0.1e-8), lo);
+          sLo[q * G::NS + c] = lo;
+          sHi[q * G::NS + c] = hi;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- phase 2: face fluxes ------------------------------------------------------
+    unsigned mood_resets = 0;
+    for (int f = tid; f < G::NFX + G::NFY; f += NT) {
+      const bool ydir = f >= G::NFX;
+      const int ff = ydir ? f - G::NFX : f;
+      const int li = ydir ? ff % G::FYW : ff % G::FXW;
+      const int lj = ydir ? ff / G::FYW : ff / G::FXW;
+      const int sa = lj * G::SX + li;                       // low cell in the slope grid
+      const int sb = sa + (ydir ? G::SX : 1);                // high cell
+      const int pa = (lj + 1) * G::PX + (li + 1);             // low cell in the primitive grid
+      const int pb = pa + (ydir ? G::PX : 1);
+      const R hh = R(ydir ? g.hy : g.hx);
+      const int d = ydir ? 1 : 0;
+      R L[6], Rv[6];
+      bool reset = false;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const R f0 = sP[q * G::NP + pa], fp = sP[q * G::NP + pb];
+        R vL = f0 + hh * sS[(2 * q + d) * G::NS + sa];
+        R vR = fp - hh * sS[(2 * q + d) * G::NS + sb];
+        if (mood_on) {   // bounds of the LOW cell, reset to its value (src/mhd_derivatives.f90:213-216)
+          const R lo = sLo[q * G::NS + sa], hi = sHi[q * G::NS + sa];
+          if (vL < lo || vL > hi) { vL = f0; reset = true; }
+          if (vR < lo || vR > hi) { vR = f0; reset = true; }
+        }
+        if (q == 0 || q == 3) {
+          vL = fmaxf(vL, R(1.0e-8));
+          vR = fmaxf(vR, R(1.0e-8));
+        }
+        L[q] = vL; Rv[q] = vR;
+      }
+      if (L[3] - R(0.5) * (L[4] * L[4] + L[5] * L[5]) < K<R>::P_floor) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) L[q] = sP[q * G::NP + pa];
+      }
+      if (Rv[3] - R(0.5) * (Rv[4] * Rv[4] + Rv[5] * Rv[5]) < K<R>::P_floor) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) Rv[q] = sP[q * G::NP + pa];
+      }
+      mood_resets += reset ? 1u : 0u;
+      const R unL = ydir ? L[2] : L[1], unR = ydir ? Rv[2] : Rv[1];
+      const R utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
+      const R bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
+      const R btL = ydir ? L[4] : L[5], btR = ydir ? Rv[4] : Rv[5];
+      Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
+      R* dst = ydir ? sFy : sFx;
+      const int NF = ydir ? G::NFY : G::NFX;
+      dst[0 * NF + ff] = F.mass;
+      dst[1 * NF + ff] = ydir ? F.momt : F.momn;
+      dst[2 * NF + ff] = ydir ? F.momn : F.momt;
+      dst[3 * NF + ff] = F.energy;
+      dst[4 * NF + ff] = F.bt;
+    }
+    if (a.counters && !a.dry) {
+      unsigned s = __reduce_add_sync(0xffffffffu, mood_resets);
+      if ((tid & 31) == 0 && s) atomicAdd(&ctl->mood_resets, (unsigned long long)s);
+    }
+    __syncthreads();
+
+    // ---- phase 3a: constrained transport -> new face B ----------------------------
+    const R* FByX = sFx + 4 * G::NFX;
+    const R* FBxY = sFy + 4 * G::NFY;
+    auto Ez = [&](int ci, int cj) -> R {
+      const int xi = (cj - j0 + 1) * G::FXW + (ci - i0 + 1);
+      const R fa = FByX[xi];
+      const R up = (cj == ny - 1 && !py) ? fa : FByX[xi + G::FXW];
+      const int yi = (cj - j0 + 1) * G::FYW + (ci - i0 + 1);
+      const R fb = FBxY[yi];
+      const R right = (ci == nx - 1 && !px) ? fb : FBxY[yi + 1];
+      return R(0.25) * (((-fa - up) + fb) + right);
+    };
+    const int bx_lo = (STAGE == 3 && (i0 > 0 || px)) ? -1 : 0;
+    const int by_lo = (STAGE == 3 && (j0 > 0 || py)) ? -1 : 0;
+    for (int e = tid; e < G::NBX + G::NBY; e += NT) {
+      const bool isy = e >= G::NBX;
+      const int ee = isy ? e - G::NBX : e;
+      int li, lj;
+      if (!isy) { li = ee % G::BXW - 1; lj = ee / G::BXW; }
+      else { li = ee % G::BYW; lj = ee / G::BYW - 1; }
+      const int i = i0 + li, j = j0 + lj;
+      if ((!isy && li < bx_lo) || (isy && lj < by_lo)) continue;
+      if (i >= nx || j >= ny) continue;
+      const int gi = (i < 0) ? i + nx : i;
+      const int gj = (j < 0) ? j + ny : j;
+      const size_t idx = size_t(gj) * nx + gi;
+      R val;
+      if (!isy) {
+        const R e0 = Ez(i, j);
+        R dbx;
+        if (j > 0 || py) dbx = ((-e0) - (-Ez(i, j - 1))) * inv_dy;
+        else dbx = ((-Ez(i, 1)) - (-e0)) * inv_dy;
+        val = in[4][idx] + dt * dbx;
+        if (STAGE == 2) val = R(0.75) * u0[4][idx] + R(0.25) * val;
+        if (STAGE == 3) val = R(1.0 / 3.0) * u0[4][idx] + R(2.0 / 3.0) * val;
+        sBx[lj * G::BXW + (li + 1)] = val;
+      } else {
+        const R e0 = Ez(i, j);
+        R dby;
+        if (i > 0 || px) dby = -(((-e0) - (-Ez(i - 1, j))) * inv_dx);
+        else dby = -(((-Ez(1, j)) - (-e0)) * inv_dx);
+        val = in[5][idx] + dt * dby;
+        if (STAGE == 2) val = R(0.75) * u0[5][idx] + R(0.25) * val;
+        if (STAGE == 3) val = R(1.0 / 3.0) * u0[5][idx] + R(2.0 / 3.0) * val;
+        sBy[(lj + 1) * G::BYW + li] = val;
+      }
+    }
+    __syncthreads();
+
+    // ---- phase 3b: cell update --------------------------------------------------------
+    double e_speed = 0.0, e_dmax = 0.0, e_dsum = 0.0, e_bmax = 0.0, e_mass = 0.0, e_en = 0.0;
+    unsigned floor_hits = 0;
+    const R ax = dt * R(g.dy);
+    const R ay = dt * R(g.dx);
+    for (int c = tid; c < TX * TY; c += NT) {
+      const int li = c % TX, lj = c / TX;
+      const int i = i0 + li, j = j0 + lj;
+      if (i >= nx || j >= ny) continue;
+      const size_t idx = size_t(j) * nx + i;
+      const int fxr = (lj + 1) * G::FXW + (li + 1);
+      const int fyt = (lj + 1) * G::FYW + (li + 1);
+      R U[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        R F = in[q][idx];
+        const R* fx = sFx + q * G::NFX;
+        const R* fy = sFy + q * G::NFY;
+        if (i > 0 || px) F = (F - ax * fx[fxr]) + ax * fx[fxr - 1];
+        else F = F - ax * fx[fxr];
+        if (j > 0 || py) F = (F - ay * fy[fyt]) + ay * fy[fyt - G::FYW];
+        else F = F - ay * fy[fyt];
+        U[q] = F;
+      }
+      const int pc = (lj + 2) * G::PX + (li + 2);
+      const R cr = sP[0 * G::NP + pc], cu = sP[1 * G::NP + pc], cv = sP[2 * G::NP + pc];
+      const R cP = sP[3 * G::NP + pc], cBx = sP[4 * G::NP + pc], cBy = sP[5 * G::NP + pc];
+      floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
+      if (!px && i == 0) {
+        const R hb = R(0.5) * (cBx * cBx + cBy * cBy);
+        const R en = ((cP - hb) / (gamma - R(1)) + R(0.5) * cr * (cu * cu + cv * cv)) + hb;
+        U[0] = U[0] + ax * cr * cu;
+        U[1] = U[1] + ax * ((cr * (cu * cu) + cP) - cBx * cBx);
+        U[2] = U[2] + ax * (cr * cu * cv - cBx * cBy);
+        U[3] = U[3] + ax * ((en + cP) * cu - cBx * (cBx * cu + cBy * cv));
+      }
+      if (!py && j == 0) {
+        const R hb = R(0.5) * (cBx * cBx + cBy * cBy);
+        const R en = ((cP - hb) / (gamma - R(1)) + R(0.5) * cr * (cu * cu + cv * cv)) + hb;
+        U[0] = U[0] + ay * cr * cv;
+        U[2] = U[2] + ay * ((cr * (cv * cv) + cP) - cBy * cBy);
+        U[1] = U[1] + ay * (cr * cv * cu - cBy * cBx);
+        U[3] = U[3] + ay * ((en + cP) * cv - cBy * (cBy * cv + cBx * cu));
+      }
+      if (STAGE == 2) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) U[q] = R(0.75) * u0[q][idx] + R(0.25) * U[q];
+      }
+      if (STAGE == 3) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) U[q] = R(1.0 / 3.0) * u0[q][idx] + R(2.0 / 3.0) * U[q];
+      }
+      if (STAGE >= 2) floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
+      const R bxn = sBx[lj * G::BXW + (li + 1)];
+      const R byn = sBy[(lj + 1) * G::BYW + li];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) out[q][idx] = U[q];
+      out[4][idx] = bxn;
+      out[5][idx] = byn;
+
+      if (STAGE == 3) {
+        const R bxm = sBx[lj * G::BXW + li];
+        const R bym = sBy[lj * G::BYW + li];
+        const bool hx = (i > 0) || px, hy = (j > 0) || py;
+        const R Bx = hx ? R(0.5) * (bxn + bxm) : bxn;
+        const R By = hy ? R(0.5) * (byn + bym) : byn;
+        const Prim<R> pr = get_primitive_mixed(U[0], U[1], U[2], U[3], Bx, By, g.gamma, g.inv_vol,
+                                               float(g.inv_vol));
+        const R inv_rho = R(1) / pr.rho;
+        const R B2 = Bx * Bx + By * By;
+        R cf = sqrtf(gamma * (pr.P - R(0.5) * B2) * inv_rho + B2 * inv_rho);
+        if (pr.rho < R(1.0e-3)) cf = fminf(cf, R(50));
+        e_speed = fmax(e_speed, double(cf + sqrtf(pr.vx * pr.vx + pr.vy * pr.vy)));
+        const double dv = fabs(divb_cell(double(bxn), double(bxm), double(byn), double(bym), hx, hy,
+                                         g.inv_dx, g.inv_dy, g.square != 0));
+        e_dmax = fmax(e_dmax, dv);
+        e_dsum += dv;
+        e_bmax = fmax(e_bmax, double(sqrtf(B2)));
+        e_mass += double(U[0]);
+        e_en += double(U[3]);
+      }
+    }
+    if (a.counters && !a.dry) {
+      unsigned s = __reduce_add_sync(0xffffffffu, floor_hits);
+      if ((tid & 31) == 0 && s) atomicAdd(&ctl->floor_hits, (unsigned long long)s);
+    }
+
+    if (STAGE == 3 && !a.dry) {
+      const double r0 = block_reduce_max<NT>(e_speed, red);
+      const double r1 = block_reduce_max<NT>(e_dmax, red);
+      const double r2 = block_reduce_sum<NT>(e_dsum, red);
+      const double r3 = block_reduce_max<NT>(e_bmax, red);
+      const double r4 = block_reduce_sum<NT>(e_mass, red);
+      const double r5 = block_reduce_sum<NT>(e_en, red);
+      if (tid == 0) {
+        double* p = a.partials + size_t(w) * NPART;
+        p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = r5;
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
+        s_last = (prev == unsigned(g.tiles_x * g.tiles_y - 1)) ? 1 : 0;
+      }
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        member_finish<NT>(g, ctl, a.partials, g.tiles_x * g.tiles_y, true, red);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace chimera
