@@ -52,6 +52,46 @@ template <int TX, int TY> struct TileGeom {
   }
 };
 
+// L2 prefetch of the input rows the CTA's NEXT tile (work item w_next) will
+// read: the conserved fields over [i0-3, i0+TX+2) x [j0-3, j0+TY+2) of the
+// stage input and, for stages 2 and 3, U^n over the tile (+1 halo face).
+// Issued at the start of the current tile so the next tile's phase-1 loads
+// hit L2 instead of HBM.  Pure hints: no result, no synchronisation.
+template <typename R, int TX, int TY, int NT, int STAGE>
+__device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_next) {
+  if (w_next >= a.total_tiles) return;
+  const int m = (a.n_members == 1) ? 0 : a.tile_member[w_next];
+  const Member& g = a.members[m];
+  const Control* ctl = a.ctl + m;
+  const int nx = g.nx, ny = g.ny;
+  const int lt = w_next - g.tile_begin;
+  const int i0 = (lt % g.tiles_x) * TX, j0 = (lt / g.tiles_x) * TY;
+  const int sbuf = ctl->parity, obuf = 1 - sbuf;
+  const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
+  const int c0 = max(i0 - 3, 0), c1 = min(i0 + TX + 2, nx) - 1;
+  constexpr int LPR = ((TX + 5) * int(sizeof(R)) + 127) / 128 + 1;   // 128-B lines per row
+  constexpr int ROWS = TY + 5;
+  constexpr int ITEMS = 6 * ROWS * LPR;
+  constexpr int ITEMS0 = (STAGE >= 2) ? 6 * (TY + 1) * LPR : 0;
+  for (int it = threadIdx.x; it < ITEMS + ITEMS0; it += NT) {
+    const bool u0 = it >= ITEMS;
+    const int k = u0 ? it - ITEMS : it;
+    const int rows = u0 ? TY + 1 : ROWS;
+    const int q = k / (rows * LPR);
+    const int rem = k - q * rows * LPR;
+    const int r = rem / LPR, l = rem - (rem / LPR) * LPR;
+    const int gj = map_index((u0 ? j0 - 1 : j0 - 3) + r, ny, g.periodic_y);
+    const char* row = reinterpret_cast<const char*>(g.buf[u0 ? sbuf : in_buf][q]) + size_t(gj) * nx * sizeof(R);
+    const char* a0 = row + size_t(u0 ? max(i0 - 1, 0) : c0) * sizeof(R);
+    const char* a1 = row + size_t(u0 ? min(i0 + TX, nx) - 1 : c1) * sizeof(R);
+    // line l of the segment; line 0 starts at a0 itself so no address precedes the row
+    const char* pl = (l == 0) ? a0
+                              : reinterpret_cast<const char*>((reinterpret_cast<uintptr_t>(a0) & ~uintptr_t(127)) +
+                                                              size_t(l) * 128);
+    if (pl <= a1) asm volatile("prefetch.global.L2 [%0];" ::"l"(pl));
+  }
+}
+
 // Block-wide reductions (deterministic for a fixed block size).
 template <int NT>
 __device__ __forceinline__ double block_reduce_sum(double v, double* red) {
@@ -229,12 +269,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
       else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
       if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
       else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
-      Prim<R> pr;
-      if constexpr (sizeof(R) == 4)
-        pr = get_primitive_mixed(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, g.gamma,
-                                 g.inv_vol, float(g.inv_vol));
-      else
-        pr = get_primitive<R>(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, gamma, vol);
+      Prim<R> pr = get_primitive<R>(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By, gamma, vol);
       sP[0 * G::NP + p] = pr.rho;
       sP[1 * G::NP + p] = pr.vx;
       sP[2 * G::NP + p] = pr.vy;

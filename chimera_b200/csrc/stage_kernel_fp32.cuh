@@ -25,6 +25,15 @@ template <int TX, int TY> struct TileGeom32 : TileGeom<TX, TY> {
   }
 };
 
+// SSP-RK3 blends (src/main.f90:202-207, 261-266) written as U0 + c (U - U0):
+// in FP32 the reference's form (1/3) U0 + (2/3) U has float(1/3) + float(2/3)
+// = 1 + 3e-8, a systematic 3e-8 gain of every conserved total per step; this
+// form conserves exactly what the stage update conserves.
+template <int STAGE>
+__device__ __forceinline__ float rk_blend(float u0, float u) {
+  return (STAGE == 2) ? u0 + 0.25f * (u - u0) : u0 + (2.0f / 3.0f) * (u - u0);
+}
+
 template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   using G = TileGeom32<TX, TY>;
@@ -71,28 +80,50 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       u0[q] = reinterpret_cast<const R*>(g.buf[sbuf][q]);
       out[q] = reinterpret_cast<R*>(g.buf[out_buf][q]);
     }
+    prefetch_next_tile<R, TX, TY, NT, STAGE>(a, w + gridDim.x);
 
     // ---- phase 1: primitives (FP64 pressure recovery) -------------------------
-    for (int p = tid; p < G::NP; p += NT) {
-      const int qx = p % G::PX, qy = p / G::PX;
-      const int si = map_index(i0 - 2 + qx, nx, px);
-      const int sj = map_index(j0 - 2 + qy, ny, py);
-      const size_t idx = size_t(sj) * nx + si;
-      const R bxc = in[4][idx];
-      const R byc = in[5][idx];
-      R Bx, By;
-      if (si > 0) Bx = R(0.5) * (bxc + in[4][idx - 1]);
-      else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
-      if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
-      else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
-      const Prim<R> pr = get_primitive_mixed(in[0][idx], in[1][idx], in[2][idx], in[3][idx], Bx, By,
-                                             g.gamma, g.inv_vol, float(g.inv_vol));
-      sP[0 * G::NP + p] = pr.rho;
-      sP[1 * G::NP + p] = pr.vx;
-      sP[2 * G::NP + p] = pr.vy;
-      sP[3 * G::NP + p] = pr.P;
-      sP[4 * G::NP + p] = pr.Bx;
-      sP[5 * G::NP + p] = pr.By;
+    {
+      // all of this thread's loads are issued before any arithmetic (memory-level parallelism)
+      constexpr int KP = (G::NP + NT - 1) / NT;
+      R ld[KP][8];
+#pragma unroll
+      for (int k = 0; k < KP; ++k) {
+        const int p = tid + k * NT;
+        if (p < G::NP) {
+          const int qx = p % G::PX, qy = p / G::PX;
+          const int si = map_index(i0 - 2 + qx, nx, px);
+          const int sj = map_index(j0 - 2 + qy, ny, py);
+          const size_t idx = size_t(sj) * nx + si;
+          const size_t ixm = (si > 0) ? idx - 1 : (px ? idx + (nx - 1) : idx);
+          const size_t iym = (sj > 0) ? idx - nx : (py ? idx + size_t(ny - 1) * nx : idx);
+          ld[k][0] = in[0][idx]; ld[k][1] = in[1][idx]; ld[k][2] = in[2][idx]; ld[k][3] = in[3][idx];
+          ld[k][4] = in[4][idx]; ld[k][5] = in[4][ixm]; ld[k][6] = in[5][idx]; ld[k][7] = in[5][iym];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < KP; ++k) {
+        const int p = tid + k * NT;
+        if (p < G::NP) {
+          const int qx = p % G::PX, qy = p / G::PX;
+          const int si = map_index(i0 - 2 + qx, nx, px);
+          const int sj = map_index(j0 - 2 + qy, ny, py);
+          const R Bx = (si > 0 || px) ? R(0.5) * (ld[k][4] + ld[k][5]) : ld[k][4];
+          const R By = (sj > 0 || py) ? R(0.5) * (ld[k][6] + ld[k][7]) : ld[k][6];
+          Prim<R> pr;
+          if constexpr (sizeof(R) == 4)
+            pr = get_primitive_mixed(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, g.gamma, g.inv_vol,
+                                     float(g.inv_vol));
+          else
+            pr = get_primitive<R>(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, gamma, vol);
+          sP[0 * G::NP + p] = pr.rho;
+          sP[1 * G::NP + p] = pr.vx;
+          sP[2 * G::NP + p] = pr.vy;
+          sP[3 * G::NP + p] = pr.P;
+          sP[4 * G::NP + p] = pr.Bx;
+          sP[5 * G::NP + p] = pr.By;
+        }
+      }
     }
     __syncthreads();
 
@@ -226,8 +257,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         if (j > 0 || py) dbx = ((-e0) - (-Ez(i, j - 1))) * inv_dy;
         else dbx = ((-Ez(i, 1)) - (-e0)) * inv_dy;
         val = in[4][idx] + dt * dbx;
-        if (STAGE == 2) val = R(0.75) * u0[4][idx] + R(0.25) * val;
-        if (STAGE == 3) val = R(1.0 / 3.0) * u0[4][idx] + R(2.0 / 3.0) * val;
+        if (STAGE >= 2) val = rk_blend<STAGE>(u0[4][idx], val);
         sBx[lj * G::BXW + (li + 1)] = val;
       } else {
         const R e0 = Ez(i, j);
@@ -235,8 +265,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         if (i > 0 || px) dby = -(((-e0) - (-Ez(i - 1, j))) * inv_dx);
         else dby = -(((-Ez(1, j)) - (-e0)) * inv_dx);
         val = in[5][idx] + dt * dby;
-        if (STAGE == 2) val = R(0.75) * u0[5][idx] + R(0.25) * val;
-        if (STAGE == 3) val = R(1.0 / 3.0) * u0[5][idx] + R(2.0 / 3.0) * val;
+        if (STAGE >= 2) val = rk_blend<STAGE>(u0[5][idx], val);
         sBy[(lj + 1) * G::BYW + li] = val;
       }
     }
@@ -286,13 +315,9 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         U[1] = U[1] + ay * (cr * cv * cu - cBy * cBx);
         U[3] = U[3] + ay * ((en + cP) * cv - cBy * (cBy * cv + cBx * cu));
       }
-      if (STAGE == 2) {
+      if (STAGE >= 2) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) U[q] = R(0.75) * u0[q][idx] + R(0.25) * U[q];
-      }
-      if (STAGE == 3) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) U[q] = R(1.0 / 3.0) * u0[q][idx] + R(2.0 / 3.0) * U[q];
+        for (int q = 0; q < 4; ++q) U[q] = rk_blend<STAGE>(u0[q][idx], U[q]);
       }
       if (STAGE >= 2) floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
       const R bxn = sBx[lj * G::BXW + (li + 1)];
