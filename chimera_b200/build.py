@@ -27,6 +27,7 @@ UNITS = {
     "kernels_fp32.cu": ["-use_fast_math"],
     "chimera_api.cu": [],
     "noalloc.cu": ["--fmad=false"],
+    "adjoint.cu": ["--fmad=false"],
 }
 
 

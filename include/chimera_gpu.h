@@ -180,6 +180,23 @@ int chimera_variant_count(chimera_handle* h);
 int chimera_set_variant(chimera_handle* h, int variant);
 int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_y, int* threads);
 
+/* ---- discrete adjoint of one RK3 step (FP64, periodic) -------------------------
+ * No counterpart in the reference.  lambda_n = (dU_{n+1}/dU_n)^T lambda_{n+1}
+ * for the step U_n -> U_{n+1} with a given (frozen) dt: the MOOD, floor and
+ * thermal-check decisions are the forward's, and at a kink the derivative is
+ * that of the branch the forward took.  Pointer arguments are arrays of six
+ * device pointers (Mass, Momx, Momy, Energy, b_x, b_y), each a dense (nx, ny)
+ * array.  All calls synchronise the adjoint's stream. */
+typedef struct chimera_adjoint chimera_adjoint;
+int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chimera_adjoint** out);
+int chimera_adjoint_step(chimera_adjoint* a, const double* const* U_n, double dt,
+                         const double* const* lambda_next, double* const* lambda_n);
+/* The same step forward with a given dt (bit-identical to chimera_step's FP64
+ * stage kernels): recomputation from checkpoints and frozen-dt replays. */
+int chimera_adjoint_forward_step(chimera_adjoint* a, const double* const* U_n, double dt,
+                                 double* const* U_next);
+void chimera_adjoint_destroy(chimera_adjoint* a);
+
 /* ---- one step without device allocation ---------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc --
  * a host code whose device memory is all owned by its own allocator, a time

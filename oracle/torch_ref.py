@@ -128,8 +128,47 @@ def fill_ghost_cells(cfg, f):
     return torch.cat([brow, mid, trow], dim=0)
 
 
-# src/mhd_derivatives.f90:50-127
+class _LimiterKinkConvention(torch.autograd.Function):
+    """Forward: the limiter value.  Backward: its derivative, except where a
+    one-sided difference is exactly zero (not differentiable there): both zero
+    -> (1/2, 1/2), one zero -> 1 w.r.t. the zero one and 0 w.r.t. the other --
+    the kink convention the GPU adjoint states."""
+
+    @staticmethod
+    def forward(ctx, dfL, dfR, limiter):
+        with torch.enable_grad():
+            a = dfL.detach().requires_grad_()
+            b = dfR.detach().requires_grad_()
+            s = _limit_plain(a, b, limiter)
+        ga, gb = torch.autograd.grad(s, (a, b), torch.ones_like(s), allow_unused=True)
+        ga = torch.zeros_like(a) if ga is None else ga
+        gb = torch.zeros_like(b) if gb is None else gb
+        zl, zr = dfL == 0.0, dfR == 0.0
+        both = zl & zr
+        ga = torch.where(both, torch.full_like(ga, 0.5), torch.where(zl, torch.ones_like(ga),
+                         torch.where(zr, torch.zeros_like(ga), ga)))
+        gb = torch.where(both, torch.full_like(gb, 0.5), torch.where(zr, torch.ones_like(gb),
+                         torch.where(zl, torch.zeros_like(gb), gb)))
+        ctx.save_for_backward(ga, gb)
+        return s.detach()
+
+    @staticmethod
+    def backward(ctx, g):
+        ga, gb = ctx.saved_tensors
+        return g * ga, g * gb, None
+
+
+KINK_CONVENTION = False   # set by the adjoint tests
+
+
 def _limit(dfL, dfR, limiter):
+    if KINK_CONVENTION and (dfL.requires_grad or dfR.requires_grad):
+        return _LimiterKinkConvention.apply(dfL, dfR, limiter)
+    return _limit_plain(dfL, dfR, limiter)
+
+
+# src/mhd_derivatives.f90:50-127
+def _limit_plain(dfL, dfR, limiter):
     prod = dfL * dfR
     den = dfL + dfR
     zero = (prod <= 0.0) | (torch.abs(den) < 1e-12)
