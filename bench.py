@@ -78,6 +78,61 @@ def profile_traffic(key):
 
 
 class Clocks:
+    """SM clock and clock-event reasons sampled DURING the timed region: an
+    NVML poll every ~2 ms on a background thread (read-only queries), so that
+    even short regions get samples; nvidia-smi (200 ms) if NVML is missing."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.smax = None
+        self._stop = None
+        self._thread = None
+        self._smi = None
+
+    def start(self):
+        import threading
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            self._stop = threading.Event()
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((float(sm), [k for k, b in bits.items() if r & b]))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.002)
+
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._smi = _SmiClocks(self.index)
+            self._smi.start()
+
+    def stop(self):
+        if self._smi is not None:
+            return self._smi.stop()
+        if self._thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self._stop.set()
+        self._thread.join(timeout=2)
+        sm = [x for x, _ in self.samples]
+        reasons = sorted({r for _, rs in self.samples for r in rs})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                "reasons": reasons, "samples": len(sm), "source": "nvml"}
+
+
+class _SmiClocks:
     """nvidia-smi samples (200 ms) during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -126,7 +181,7 @@ class Clocks:
                         reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def dist_setup(args):
@@ -335,14 +390,21 @@ def run_ensemble(args, world):
     from chimera_b200 import ensemble
     from chimera_b200.config import FP32_BULK, FP64
 
+    from chimera_b200 import problems
+    from chimera_b200.shard import shard_members
+
     steps = args.ens_steps
     graph = 10 if steps % 10 == 0 else 1
     res = {}
     finals = {}
     hbm, _ = peaks()
+    rank = int(os.environ.get("RANK", "0"))
+    sizes = problems.grf_ensemble_sizes(args.ens_scale)
+    all_cells = sum(n * n for n in sizes)
+    mine = set(shard_members([n * n for n in sizes], world, rank))   # members are independent: no exchange
     for name, prec in (("fp32_batched", FP32_BULK), ("fp64_batched", FP64)):
-        cfgs, states = ensemble.grf_ensemble(args.ens_scale, prec)
-        cells = ensemble.cells(cfgs)
+        cfgs, states = ensemble.grf_ensemble(args.ens_scale, prec, members=mine)
+        cells = all_cells
         s = ensemble.make_batch(cfgs, states)
         s.step(1)
         if args.ens_variant >= 0:
@@ -371,11 +433,13 @@ def run_ensemble(args, world):
         e1.synchronize()
         ms = dist_max(e0.elapsed_time(e1), world)
         esize = 4 if prec == FP32_BULK else 8
-        zcs = world * cells * steps / (ms * 1e-3)
+        zcs = cells * steps / (ms * 1e-3)
         res[name] = {"value": zcs, "unit": "zone-cycles/s", "ms": ms, "steps": steps,
-                     "members": len(cfgs), "cells": cells, "tile": s.variant(),
+                     "members": len(sizes), "members_per_rank_max": len(cfgs), "cells": cells,
+                     "tile": s.variant(),
                      "bytes_per_zone_cycle": 48 * esize,
                      "hbm_fraction": zcs / world * 48 * esize / (hbm * 1e9),
+                     "scaling": "strong (members sharded across ranks)",
                      "graph_steps": graph}
         finals[name] = [s.get_state(member=m) for m in range(len(cfgs))]
         s.close()
@@ -385,6 +449,11 @@ def run_ensemble(args, world):
         for q in range(6):
             num[q] += np.sum(np.abs(a[q] - b[q]))
             den[q] += np.sum(np.abs(b[q]))
+    if world > 1:   # diagnostics only
+        import torch.distributed as dist
+        t = torch.tensor(np.concatenate([num, den]), dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        num, den = t[:6].cpu().numpy(), t[6:].cpu().numpy()
     l1 = (num / den).tolist()
     res["fp32_l1_vs_fp64"] = dict(zip(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y"), l1))
     res["fp32_over_fp64"] = res["fp32_batched"]["value"] / res["fp64_batched"]["value"]

@@ -11,12 +11,16 @@ from . import problems
 from .config import FP32_BULK, FP64
 
 
-def grf_ensemble(scale: int = 1, precision: int = FP32_BULK, seed0: int = 1000):
+def grf_ensemble(scale: int = 1, precision: int = FP32_BULK, seed0: int = 1000, members=None):
     """Configs and conserved states of the GRF ensemble: 256 members at 128^2,
     192 at 256^2, 64 at 512^2 (``scale`` divides the member counts).  Member k
-    is seeded with ``seed0 + k`` (Philox)."""
+    is seeded with ``seed0 + k`` (Philox).  ``members`` selects a subset of
+    member indices (a rank's shard)."""
     cfgs, states = [], []
-    for k, n in enumerate(problems.grf_ensemble_sizes(scale)):
+    sizes = problems.grf_ensemble_sizes(scale)
+    for k, n in enumerate(sizes):
+        if members is not None and k not in members:
+            continue
         cfg, st = problems.grf_member(n, seed0 + k)
         cfgs.append(cfg.replace(precision=precision))
         states.append(st)
