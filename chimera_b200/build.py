@@ -28,6 +28,7 @@ UNITS = {
     "chimera_api.cu": [],
     "noalloc.cu": ["--fmad=false"],
     "adjoint.cu": ["--fmad=false"],
+    "unit_ops.cu": ["--fmad=false"],
 }
 
 

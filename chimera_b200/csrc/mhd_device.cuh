@@ -54,6 +54,19 @@ __device__ __forceinline__ Prim<R> get_primitive(R M, R Mx, R My, R E, R Bx, R B
   return p;
 }
 
+// src/mhd_change_states.f90:16-58 (get_conserved), one cell.
+template <typename R>
+__device__ __forceinline__ void get_conserved(R rho, R vx, R vy, R P, R Bx, R By, R gamma, R vol, R& M, R& Mx,
+                                              R& My, R& E) {
+  const R rho_cp = dmax(rho, K<R>::rho_floor);
+  const R P_cp = dmax(P, K<R>::P_floor);
+  M = rho_cp * vol;
+  Mx = M * vx;
+  My = M * vy;
+  const R halfB2 = R(0.5) * (Bx * Bx + By * By);
+  E = (((P_cp - halfB2) / (gamma - R(1)) + R(0.5) * rho_cp * (vx * vx + vy * vy)) + halfB2) * vol;
+}
+
 // FP32-bulk form: storage and bulk arithmetic are FP32, but the pressure
 // recovery p = (gamma-1)(E/vol - rho v^2/2 - B^2/2) + B^2/2 -- a small
 // difference of large terms at low plasma beta -- is done in FP64 from the

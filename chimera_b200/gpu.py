@@ -115,7 +115,7 @@ def _check(rc: int, what: str) -> None:
 def to_ccfg(cfg: SolverConfig) -> CCfg:
     return CCfg(cfg.nx, cfg.ny, cfg.dx, cfg.dy, cfg.gamma, cfg.courant, cfg.t_out, cfg.t_end,
                 cfg.bc[0], cfg.bc[1], cfg.bc[2], cfg.bc[3], cfg.riemann, cfg.limiter,
-                int(bool(cfg.slope_limiting)), int(bool(cfg.mood)), int(cfg.precision))
+                int(bool(cfg.slope_limiting)), int(bool(cfg.mood)), int(getattr(cfg, "precision", 0)))
 
 
 def _ptrs(arrays, nx, ny):

@@ -221,6 +221,50 @@ int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, double* Momx,
                              double* Energy, double* b_x, double* b_y, double* t,
                              int* output_count, double* dt_next, void* stream);
 
+/* ---- the reference's module routines, one kernel each ----------------------------
+ * Same names, argument meaning and per-side boundary handling as the Fortran
+ * routines; dense (nx, ny) device arrays (x fastest), cfg gives nx, ny, dx, dy,
+ * gamma, the BC flags, riemann, limiter and mood; asynchronous on `stream`. */
+int chimera_op_average_face_to_cell_B(const chimera_cfg* cfg, const double* b_x, const double* b_y,
+                                      double* Bx, double* By, void* stream);   /* src/mhd_field_ops.f90:120-156 */
+int chimera_op_get_primitive(const chimera_cfg* cfg, const double* Mass, const double* Momx,
+                             const double* Momy, const double* Energy, const double* Bx,
+                             const double* By, double* rho, double* vx, double* vy, double* P,
+                             void* stream);                                   /* src/mhd_change_states.f90:61-113 */
+int chimera_op_get_conserved(const chimera_cfg* cfg, const double* rho, const double* vx,
+                             const double* vy, const double* P, const double* Bx, const double* By,
+                             double* Mass, double* Momx, double* Momy, double* Energy,
+                             void* stream);                                   /* src/mhd_change_states.f90:16-58 */
+int chimera_op_apply_conserved_floors(const chimera_cfg* cfg, double* Mass, double* Momx, double* Momy,
+                                      double* Energy, const double* Bx, const double* By,
+                                      void* stream);                          /* src/mhd_change_states.f90:116-166 */
+int chimera_op_fill_ghost_cells(const chimera_cfg* cfg, const double* f, double* f_pad,
+                                void* stream);            /* src/mhd_bc.f90:36-170; f_pad is (nx+2, ny+2) */
+int chimera_op_compute_gradients(const chimera_cfg* cfg, const double* f_pad, double* f_dx, double* f_dy,
+                                 void* stream);                               /* src/mhd_derivatives.f90:15-47 */
+int chimera_op_apply_slope_limiter(const chimera_cfg* cfg, const double* f_pad, double* f_dx,
+                                   double* f_dy, void* stream);               /* src/mhd_derivatives.f90:50-127 */
+int chimera_op_reconstruction(const chimera_cfg* cfg, const double* f, const double* f_dx,
+                              const double* f_dy, double* f_XL, double* f_XR, double* f_YL,
+                              double* f_YR, int rho_or_p, void* stream);      /* src/mhd_derivatives.f90:130-229 */
+/* faces24[s*6+q]: slot s in (XL, XR, YL, YR), field q in (P, Bx, By, rho, vx, vy); cell6 likewise */
+int chimera_op_thermal_pressure_check(const chimera_cfg* cfg, double* const* faces24,
+                                      const double* const* cell6, void* stream); /* src/mhd_derivatives.f90:232-293 */
+/* in12: rho_L, rho_R, vx_L, vx_R, vy_L, vy_R, P_L, P_R, Bx_L, Bx_R, By_L, By_R (normal first);
+ * out5: mass, normal momentum, tangential momentum, energy, tangential B */
+int chimera_op_compute_fluxes(const chimera_cfg* cfg, const double* const* in12, double* const* out5,
+                              void* stream);                                  /* src/mhd_flux.f90:139-779 */
+int chimera_op_update_conserved(const chimera_cfg* cfg, double* F, const double* flux_X,
+                                const double* flux_Y, double dt, void* stream); /* src/mhd_flux.f90:20-76 */
+/* scratch: one caller-owned (nx, ny) array */
+int chimera_op_constrained_transport(const chimera_cfg* cfg, double* b_x, double* b_y,
+                                     const double* flux_By_X, const double* flux_Bx_Y, double dt,
+                                     double* scratch, void* stream);          /* src/mhd_flux.f90:79-136 */
+int chimera_op_compute_curl_2d(const chimera_cfg* cfg, const double* Az, double* b_x, double* b_y,
+                               void* stream);                                 /* src/mhd_field_ops.f90:15-57 */
+int chimera_op_compute_divB(const chimera_cfg* cfg, const double* b_x, const double* b_y, double* divB,
+                            void* stream);                                    /* src/mhd_field_ops.f90:60-117 */
+
 /* ---- misc ------------------------------------------------------------------ */
 const char* chimera_strerror(int code);
 int chimera_version(void);
