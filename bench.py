@@ -52,7 +52,11 @@ def parse():
                    help="divide the ensemble member counts (1 = 256x128^2 + 192x256^2 + 64x512^2)")
     p.add_argument("--ens-steps", type=int, default=200)
     p.add_argument("--ens-variant", type=int, default=-1,
-                   help="force a tile variant for the ensemble (-1: autotune)")
+                   help="force a tile variant for the FP32-batched ensemble (-1: autotune)")
+    p.add_argument("--ens-forms", default="fp32,fp64",
+                   help="ensemble forms to measure (the L1 comparison needs both)")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="force a tile variant for the single-grid measurement (-1: autotune)")
     return p.parse_args()
 
 
@@ -277,7 +281,10 @@ def run_chimera(args, world, rank, local):
     s.set_state(st)
     ext = torch.cuda.ExternalStream(s.stream)
     s.step(args.warmup)
-    variant, tuned_ms = s.autotune(reps=3)      # tile shape for this problem (cached per shape)
+    if args.variant >= 0:
+        s.set_variant(args.variant)
+    else:
+        s.autotune(reps=3)                      # tile shape for this problem (cached per shape)
     vinfo = s.variant()
     torch.cuda.synchronize()
 
@@ -402,12 +409,14 @@ def run_ensemble(args, world):
     sizes = problems.grf_ensemble_sizes(args.ens_scale)
     all_cells = sum(n * n for n in sizes)
     mine = set(shard_members([n * n for n in sizes], world, rank))   # members are independent: no exchange
-    for name, prec in (("fp32_batched", FP32_BULK), ("fp64_batched", FP64)):
+    forms = [(n, p) for n, p in (("fp32_batched", FP32_BULK), ("fp64_batched", FP64))
+             if n.split("_")[0] in args.ens_forms.split(",")]
+    for name, prec in forms:
         cfgs, states = ensemble.grf_ensemble(args.ens_scale, prec, members=mine)
         cells = all_cells
         s = ensemble.make_batch(cfgs, states)
         s.step(1)
-        if args.ens_variant >= 0:
+        if args.ens_variant >= 0 and prec == FP32_BULK:
             s.set_variant(args.ens_variant)
         else:
             s.autotune(reps=2)
@@ -442,20 +451,36 @@ def run_ensemble(args, world):
                      "scaling": "strong (members sharded across ranks)",
                      "graph_steps": graph}
         finals[name] = [s.get_state(member=m) for m in range(len(cfgs))]
+        if prec == FP64 and "fp32_batched" in finals:
+            # conditioning of the ensemble: the same FP64 run from the initial states
+            # rounded to FP32 (untimed); the FP32 form cannot be closer than this floor
+            for m, st in enumerate(states):
+                s.set_state([a.astype(np.float32).astype(np.float64) for a in st], member=m)
+                s.set_time(0.0, 1, member=m)
+            s.step(0)
+            for _ in range(steps // graph):
+                s.step(graph)
+            finals["fp64_ic_rounded"] = [s.get_state(member=m) for m in range(len(cfgs))]
         s.close()
-    num = np.zeros(6)
-    den = np.zeros(6)
-    for a, b in zip(finals["fp32_batched"], finals["fp64_batched"]):
-        for q in range(6):
-            num[q] += np.sum(np.abs(a[q] - b[q]))
-            den[q] += np.sum(np.abs(b[q]))
-    if world > 1:   # diagnostics only
-        import torch.distributed as dist
-        t = torch.tensor(np.concatenate([num, den]), dtype=torch.float64, device="cuda")
-        dist.all_reduce(t)
-        num, den = t[:6].cpu().numpy(), t[6:].cpu().numpy()
-    l1 = (num / den).tolist()
-    res["fp32_l1_vs_fp64"] = dict(zip(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y"), l1))
+    if "fp32_batched" not in finals or "fp64_batched" not in finals:
+        return res
+
+    def l1_vs_fp64(key):
+        num = np.zeros(6)
+        den = np.zeros(6)
+        for a, b in zip(finals[key], finals["fp64_batched"]):
+            for q in range(6):
+                num[q] += np.sum(np.abs(a[q] - b[q]))
+                den[q] += np.sum(np.abs(b[q]))
+        if world > 1:   # diagnostics only
+            import torch.distributed as dist
+            t = torch.tensor(np.concatenate([num, den]), dtype=torch.float64, device="cuda")
+            dist.all_reduce(t)
+            num, den = t[:6].cpu().numpy(), t[6:].cpu().numpy()
+        return dict(zip(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y"), (num / den).tolist()))
+
+    res["fp32_l1_vs_fp64"] = l1_vs_fp64("fp32_batched")
+    res["fp64_from_fp32_rounded_ic_l1_vs_fp64"] = l1_vs_fp64("fp64_ic_rounded")
     res["fp32_over_fp64"] = res["fp32_batched"]["value"] / res["fp64_batched"]["value"]
     res["workload"] = (f"GRF ensemble, {res['fp32_batched']['members']} members of uneven sizes "
                        f"(128^2/256^2/512^2), periodic, Rusanov + MC + MOOD, {steps} RK3 steps")

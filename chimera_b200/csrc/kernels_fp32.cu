@@ -7,11 +7,11 @@
 namespace chimera {
 
 namespace {
-template <int TX, int TY, int NT, int MINB>
+template <int TX, int TY, int NT, int MINB, bool SB = true>
 void fill(KernelSet* ks) {
-  const size_t smem = TileGeom32<TX, TY>::smem_bytes();
+  const size_t smem = TileGeom32<TX, TY, SB>::smem_bytes();
 #define CHIMERA_ENTRY(S, K) \
-  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB>, smem, TX, TY, NT}
+  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB>, smem, TX, TY, NT}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
@@ -22,7 +22,7 @@ void fill(KernelSet* ks) {
 }  // namespace
 
 // Tile shapes and occupancy targets the autotuner chooses from.
-int fp32_variant_count() { return 5; }
+int fp32_variant_count() { return 9; }
 
 void fp32_kernels(int variant, KernelSet* out) {
   switch (variant) {
@@ -30,6 +30,10 @@ void fp32_kernels(int variant, KernelSet* out) {
     case 2: fill<64, 8, 256, 2>(out); break;
     case 3: fill<16, 16, 128, 4>(out); break;
     case 4: fill<32, 16, 512, 1>(out); break;
+    case 5: fill<32, 16, 256, 3, false>(out); break;
+    case 6: fill<16, 16, 128, 6, false>(out); break;
+    case 7: fill<32, 8, 128, 5, false>(out); break;
+    case 8: fill<64, 8, 256, 2, false>(out); break;
     default: fill<32, 16, 256, 2>(out); break;
   }
 }

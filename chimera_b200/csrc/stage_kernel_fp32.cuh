@@ -16,12 +16,16 @@
 
 namespace chimera {
 
-template <int TX, int TY> struct TileGeom32 : TileGeom<TX, TY> {
+// Shared-memory plan.  SB: MOOD bounds stored per cell (12 arrays) or
+// recomputed per face from the primitives.  The new face-B arrays of phase 3a
+// reuse the slope arrays, which are dead once the face fluxes exist.
+template <int TX, int TY, bool SB> struct TileGeom32 : TileGeom<TX, TY> {
   using B = TileGeom<TX, TY>;
   static constexpr int SX = TX + 2, SY = TY + 2, NS = SX * SY;   // cells [i0-1, i0+TX] x [j0-1, j0+TY]
+  static constexpr int NSA = SB ? 24 : 12;                       // per-cell arrays: slopes (+ bounds)
+  static_assert(B::NBX + B::NBY <= 12 * NS, "face-B arrays must fit in the slope arrays");
   static constexpr size_t smem_bytes() {
-    return sizeof(float) * (size_t(6) * B::NP + size_t(24) * NS + size_t(5) * B::NFX + size_t(5) * B::NFY +
-                            B::NBX + B::NBY);
+    return sizeof(float) * (size_t(6) * B::NP + size_t(NSA) * NS + size_t(5) * B::NFX + size_t(5) * B::NFY);
   }
 };
 
@@ -34,18 +38,18 @@ __device__ __forceinline__ float rk_blend(float u0, float u) {
   return (STAGE == 2) ? u0 + 0.25f * (u - u0) : u0 + (2.0f / 3.0f) * (u - u0);
 }
 
-template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB>
+template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
-  using G = TileGeom32<TX, TY>;
+  using G = TileGeom32<TX, TY, SB>;
   using R = float;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);       // [6][NP]   primitives, tile + 2 halo
   R* sS = sP + 6 * G::NP;                       // [12][NS]  slopes: field q, dir d at (2q+d)
-  R* sLo = sS + 12 * G::NS;                     // [6][NS]   MOOD lower bounds
-  R* sHi = sLo + 6 * G::NS;                     // [6][NS]   MOOD upper bounds
-  R* sFx = sHi + 6 * G::NS;                     // [5][NFX]
+  R* sLo = sS + 12 * G::NS;                     // [6][NS]   MOOD lower bounds (SB)
+  R* sHi = sLo + 6 * G::NS;                     // [6][NS]   MOOD upper bounds (SB)
+  R* sFx = sS + G::NSA * G::NS;                 // [5][NFX]
   R* sFy = sFx + 5 * G::NFX;                    // [5][NFY]
-  R* sBx = sFy + 5 * G::NFY;
+  R* sBx = sS;                                  // new face B (phase 3a on): reuses the slopes
   R* sBy = sBx + G::NBX;
   __shared__ double red[NT / 32];
   __shared__ int s_last;
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         }
         sS[(2 * q + 0) * G::NS + c] = sx;
         sS[(2 * q + 1) * G::NS + c] = sy;
-        if (mood_on) {
+        if (SB && mood_on) {
           R lo = fminf(fminf(fminf(fminf(f0, xp), xm), yp), ym);
           const R hi = fmaxf(fmaxf(fmaxf(fmaxf(f0, xp), xm), yp), ym);
           if (q == 0 || q == 3) lo = fmaxf(R(0.1e-8), lo);
@@ -186,7 +190,17 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         R vL = f0 + hh * sS[(2 * q + d) * G::NS + sa];
         R vR = fp - hh * sS[(2 * q + d) * G::NS + sb];
         if (mood_on) {   // bounds of the LOW cell, reset to its value (src/mhd_derivatives.f90:213-216)
-          const R lo = sLo[q * G::NS + sa], hi = sHi[q * G::NS + sa];
+          R lo, hi;
+          if (SB) {
+            lo = sLo[q * G::NS + sa];
+            hi = sHi[q * G::NS + sa];
+          } else {       // the 5-point stencil of the low cell (:190-211), as phase 1.5 forms it
+            const R* s = sP + q * G::NP;
+            const R xp = s[pa + 1], xm = s[pa - 1], yp = s[pa + G::PX], ym = s[pa - G::PX];
+            lo = fminf(fminf(fminf(fminf(f0, xp), xm), yp), ym);
+            hi = fmaxf(fmaxf(fmaxf(fmaxf(f0, xp), xm), yp), ym);
+            if (q == 0 || q == 3) lo = fmaxf(R(0.1e-8), lo);
+          }
           if (vL < lo || vL > hi) { vL = f0; reset = true; }
           if (vR < lo || vR > hi) { vR = f0; reset = true; }
         }

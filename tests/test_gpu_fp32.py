@@ -93,3 +93,36 @@ def test_fp32_batched_ensemble_vs_fp64(G):
             num[q] += np.sum(np.abs(a[q] - b[q]))
             den[q] += np.sum(np.abs(b[q]))
     assert np.max(num / den) <= 1e-5, num / den
+
+
+def _ens_l1(a_list, b_list):
+    num = np.zeros(6)
+    den = np.zeros(6)
+    for a, b in zip(a_list, b_list):
+        for q in range(6):
+            num[q] += np.sum(np.abs(a[q] - b[q]))
+            den[q] += np.sum(np.abs(b[q]))
+    return num / den
+
+
+def test_fp32_ensemble_error_is_the_conditioning_floor(G):
+    """Over 200 steps the GRF flows form shocks and small perturbations grow
+    quickly (most on the 128^2 members).  The exact FP64 solver started from
+    the initial states rounded to FP32 deviates from the exact-start run by a
+    given L1 after 200 steps; the FP32-bulk form (FP32 storage and arithmetic)
+    must stay within a factor 2 of that floor, and within 1e-5 at 100 steps.
+    (Measured on the full ensemble: both about 2.4e-5 in Momx at 200 steps.)"""
+    cfgs, states = ensemble.grf_ensemble(16, FP64)
+    rounded = [[a.astype(np.float32).astype(np.float64) for a in st] for st in states]
+    runs = {}
+    for key, prec, init in (("ref", FP64, states), ("rounded", FP64, rounded), ("fp32", FP32_BULK, states)):
+        s = ensemble.make_batch([c.replace(precision=prec) for c in cfgs], init)
+        s.step(100)
+        mid = [s.get_state(member=m) for m in range(len(cfgs))]
+        s.step(100)
+        runs[key] = (mid, [s.get_state(member=m) for m in range(len(cfgs))])
+        s.close()
+    assert np.max(_ens_l1(runs["fp32"][0], runs["ref"][0])) <= 1e-5
+    floor = _ens_l1(runs["rounded"][1], runs["ref"][1])
+    err = _ens_l1(runs["fp32"][1], runs["ref"][1])
+    assert np.all(err <= 2.0 * floor + 1e-7), (err, floor)
