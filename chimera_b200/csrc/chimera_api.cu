@@ -6,6 +6,7 @@
 // per-tile reduction partials and the (member, tile) work list; the stage
 // kernels are launched persistently over that work list, one launch per RK
 // stage, optionally replayed from a captured CUDA graph.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -23,6 +24,9 @@
 
 using namespace chimera;
 
+constexpr size_t TMAP_BYTES_HOST = sizeof(CUtensorMap);
+static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
+
 namespace {
 
 // ---- FP32-bulk conversion kernels (host <-> storage precision) ---------------
@@ -36,6 +40,40 @@ __global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__
 }
 
 bool valid_bc(int b) { return b >= CHIMERA_BC_PERIODIC && b <= CHIMERA_BC_INFLOW; }
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (the library
+// links only cudart); null if the driver does not provide it.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    cudaGetLastError();
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of one FP32 (ny, nx) field with a bw x bh box; false if the
+// field's shape does not allow one (row pitch not a multiple of 16 bytes, or
+// smaller than the box).
+bool encode_field_map(void* map, void* base, int nx, int ny, int bw, int bh) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn || nx % 4 != 0 || nx < bw || ny < bh || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  const cuuint64_t dims[2] = {cuuint64_t(nx), cuuint64_t(ny)};
+  const cuuint64_t strides[1] = {cuuint64_t(nx) * sizeof(float)};
+  const cuuint32_t box[2] = {cuuint32_t(bw), cuuint32_t(bh)};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(static_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -62,6 +100,9 @@ struct chimera_handle {
   double* d_part = nullptr;
   int* d_tile_member = nullptr;
   void* pool = nullptr;              // all state buffers
+  char* d_tmaps = nullptr;           // [TMA variant slot][member][buffer 3][field 6] tensor maps
+  std::vector<int> tmap_slot;        // per variant: its slot in d_tmaps, -1 without TMA
+  std::vector<unsigned char> tmap_ok;   // [slot][member]: the member's maps exist
   double* d_stage64 = nullptr;       // FP64 staging for FP32-bulk set/get
   size_t max_cells = 0;
   std::vector<bool> dt_valid;        // per member: Control::dt matches the state
@@ -249,6 +290,14 @@ static int layout(chimera_handle* h, int v) {
     tiles += g.tiles_x * g.tiles_y;
   }
   h->total_tiles = tiles;
+  // TMA variants: the variant's tensor maps (encoded once at creation and never
+  // modified) for the members whose shape allows them; the others, and every
+  // edge tile, use plain loads
+  const int slot = h->tmap_slot.empty() ? -1 : h->tmap_slot[v];
+  for (int m = 0; m < h->n; ++m)
+    h->hm[m].tmap = (slot >= 0 && h->tmap_ok[size_t(slot) * h->n + m])
+                        ? h->d_tmaps + (size_t(slot) * h->n + m) * 18 * TMAP_BYTES_HOST
+                        : nullptr;
   std::vector<int> tm(tiles);
   for (int m = 0; m < h->n; ++m)
     for (int k = 0; k < h->hm[m].tiles_x * h->hm[m].tiles_y; ++k) tm[h->hm[m].tile_begin + k] = m;
@@ -397,6 +446,37 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
     chimera_destroy(h);
     return CHIMERA_ERR_NOMEM;
   }
+  // tensor maps of every TMA variant, written once here and never modified
+  h->tmap_slot.assign(nv, -1);
+  int slots = 0;
+  for (int v = 0; v < nv; ++v)
+    if (h->variants[v].stage[0][0].box_w > 0) h->tmap_slot[v] = slots++;
+  if (slots > 0) {
+    const size_t per_slot = size_t(n_members) * 18 * TMAP_BYTES_HOST;
+    std::vector<unsigned char> maps(per_slot * slots, 0);
+    h->tmap_ok.assign(size_t(slots) * n_members, 0);
+    for (int v = 0; v < nv; ++v) {
+      const int sl = h->tmap_slot[v];
+      if (sl < 0) continue;
+      const int bw = h->variants[v].stage[0][0].box_w, bh = h->variants[v].stage[0][0].box_h;
+      for (int m = 0; m < n_members; ++m) {
+        const Member& g = h->hm[m];
+        bool ok = true;
+        for (int b = 0; b < 3 && ok; ++b)
+          for (int q = 0; q < 6 && ok; ++q)
+            ok = encode_field_map(&maps[sl * per_slot + (size_t(m) * 18 + b * 6 + q) * TMAP_BYTES_HOST],
+                                  g.buf[b][q], g.nx, g.ny, bw, bh);
+        h->tmap_ok[size_t(sl) * n_members + m] = ok ? 1 : 0;
+      }
+    }
+    if (cudaMalloc(&h->d_tmaps, maps.size()) != cudaSuccess ||
+        cudaMemcpyAsync(h->d_tmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      cudaGetLastError();
+      chimera_destroy(h);
+      return CHIMERA_ERR_NOMEM;
+    }
+  }
   if (h->precision == CHIMERA_FP32_BULK) {
     if (cudaMalloc(&h->d_stage64, sizeof(double) * h->max_cells) != cudaSuccess) {
       cudaGetLastError();
@@ -434,6 +514,7 @@ void chimera_destroy(chimera_handle* h) {
   cudaFree(h->d_part);
   cudaFree(h->d_tile_member);
   cudaFree(h->d_stage64);
+  cudaFree(h->d_tmaps);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   cudaGetLastError();
   delete h;

@@ -31,7 +31,8 @@ struct Member {
   double inv_vol;          // 1/vol (FP32-bulk pressure recovery)
   double courant, t_out, t_end;
   void* buf[3][6];
-  void* e64[3];            // FP32-bulk form: FP64 Energy per buffer (unused in FP64)
+  const void* tmap;        // TMA variants: this member's tensor maps [buffer 3][field 6] (CUtensorMap,
+                           // 128 bytes each, boxes of the variant's tile) in device memory, or null
 };
 
 // Time-loop state of one member, resident on the device so that whole runs

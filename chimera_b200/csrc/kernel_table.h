@@ -9,6 +9,7 @@ struct KernelEntry {
   const void* fn;      // __global__ function (host stub address)
   size_t smem;         // dynamic shared memory bytes
   int tx, ty, nt;      // tile shape and block size
+  int box_w = 0, box_h = 0;   // TMA box of the stage input (elements), 0 = plain loads
 };
 
 struct KernelSet {

@@ -7,11 +7,14 @@
 namespace chimera {
 
 namespace {
-template <int TX, int TY, int NT, int MINB, bool SB = true>
+template <int TX, int TY, int NT, int MINB, bool SB = true, bool TMA = false>
 void fill(KernelSet* ks) {
-  const size_t smem = TileGeom32<TX, TY, SB>::smem_bytes();
-#define CHIMERA_ENTRY(S, K) \
-  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB>, smem, TX, TY, NT}
+  using G = TileGeom32<TX, TY, SB>;
+  const size_t smem = G::smem_bytes();
+  const int bw = TMA ? G::BW : 0, bh = TMA ? G::BH : 0;
+#define CHIMERA_ENTRY(S, K)                                                                            \
+  ks->stage[S - 1][K - 1] =                                                                           \
+      KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB, TMA>, smem, TX, TY, NT, bw, bh}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
@@ -22,7 +25,7 @@ void fill(KernelSet* ks) {
 }  // namespace
 
 // Tile shapes and occupancy targets the autotuner chooses from.
-int fp32_variant_count() { return 9; }
+int fp32_variant_count() { return 11; }
 
 void fp32_kernels(int variant, KernelSet* out) {
   switch (variant) {
@@ -34,6 +37,8 @@ void fp32_kernels(int variant, KernelSet* out) {
     case 6: fill<16, 16, 128, 6, false>(out); break;
     case 7: fill<32, 8, 128, 5, false>(out); break;
     case 8: fill<64, 8, 256, 2, false>(out); break;
+    case 9: fill<32, 16, 256, 3, false, true>(out); break;
+    case 10: fill<16, 16, 128, 6, false, true>(out); break;
     default: fill<32, 16, 256, 2>(out); break;
   }
 }

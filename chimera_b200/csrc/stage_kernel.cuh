@@ -56,9 +56,10 @@ template <int TX, int TY> struct TileGeom {
 // read: the conserved fields over [i0-3, i0+TX+2) x [j0-3, j0+TY+2) of the
 // stage input and, for stages 2 and 3, U^n over the tile (+1 halo face).
 // Issued at the start of the current tile so the next tile's phase-1 loads
-// hit L2 instead of HBM.  Pure hints: no result, no synchronisation.
+// hit L2 instead of HBM.  Pure hints: no result, no synchronisation.  With
+// inputs = false only the U^n rows are prefetched (the inputs come by TMA).
 template <typename R, int TX, int TY, int NT, int STAGE>
-__device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_next) {
+__device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_next, bool inputs = true) {
   if (w_next >= a.total_tiles) return;
   const int m = (a.n_members == 1) ? 0 : a.tile_member[w_next];
   const Member& g = a.members[m];
@@ -73,7 +74,7 @@ __device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_nex
   constexpr int ROWS = TY + 5;
   constexpr int ITEMS = 6 * ROWS * LPR;
   constexpr int ITEMS0 = (STAGE >= 2) ? 6 * (TY + 1) * LPR : 0;
-  for (int it = threadIdx.x; it < ITEMS + ITEMS0; it += NT) {
+  for (int it = threadIdx.x + (inputs ? 0 : ITEMS); it < ITEMS + ITEMS0; it += NT) {
     const bool u0 = it >= ITEMS;
     const int k = u0 ? it - ITEMS : it;
     const int rows = u0 ? TY + 1 : ROWS;

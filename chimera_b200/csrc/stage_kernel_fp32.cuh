@@ -7,23 +7,38 @@
 //     once into shared memory; the FP64 kernel recomputes them for each face
 //     that touches the cell (twice per direction);
 //   * the translation unit is compiled with fast FP32 division and square
-//     root (-use_fast_math), about 1 ulp instead of correctly rounded.
+//     root (-use_fast_math), about 1 ulp instead of correctly rounded;
+//   * (TMA variants) the inputs of the CTA's next tile are loaded by TMA box
+//     copies into the dead slope arrays while the current tile does
+//     constrained transport and the cell update, so phase 1 reads shared
+//     memory instead of waiting on HBM.  Tiles whose box would leave the
+//     array (domain edges, where the index maps wrap or clamp) use the plain
+//     loads.
 // Kept in FP64: the pressure recovery p = (gamma-1)(E - rho v^2/2 - B^2/2)
 // (get_primitive_mixed), the CFL dt reduction and the tOut clip, and the
 // conserved-total sums.  The per-cell CFL speed is computed in FP32.
 #pragma once
 #include "stage_kernel.cuh"
+#include "tma.cuh"
 
 namespace chimera {
 
 // Shared-memory plan.  SB: MOOD bounds stored per cell (12 arrays) or
 // recomputed per face from the primitives.  The new face-B arrays of phase 3a
 // reuse the slope arrays, which are dead once the face fluxes exist.
+// TMA staging: the six input fields over the box [i0-4, i0-4+BW) x [j0-3,
+// j0-3+BH) -- the primitives' 2-cell halo plus b_x(i-1), b_y(j-1) -- with the
+// box origin's x a multiple of 4 floats (16 bytes), each field's box padded to
+// 128 bytes, placed in the slope arrays after the face-B arrays.
 template <int TX, int TY, bool SB> struct TileGeom32 : TileGeom<TX, TY> {
   using B = TileGeom<TX, TY>;
   static constexpr int SX = TX + 2, SY = TY + 2, NS = SX * SY;   // cells [i0-1, i0+TX] x [j0-1, j0+TY]
   static constexpr int NSA = SB ? 24 : 12;                       // per-cell arrays: slopes (+ bounds)
   static_assert(B::NBX + B::NBY <= 12 * NS, "face-B arrays must fit in the slope arrays");
+  static constexpr int BW = ((TX + 6 + 3) / 4) * 4, BH = TY + 5;  // TMA box (floats)
+  static constexpr int BOXF = ((BW * BH + 31) / 32) * 32;        // one field's box, 128-byte multiple
+  static constexpr int STG0 = ((B::NBX + B::NBY + 31) / 32) * 32; // staging offset in the slope arrays
+  static constexpr bool TMA_FITS = STG0 + 32 + 6 * BOXF <= 12 * NS;   // (+32: 128-byte alignment slack)
   static constexpr size_t smem_bytes() {
     return sizeof(float) * (size_t(6) * B::NP + size_t(NSA) * NS + size_t(5) * B::NFX + size_t(5) * B::NFY);
   }
@@ -38,9 +53,37 @@ __device__ __forceinline__ float rk_blend(float u0, float u) {
   return (STAGE == 2) ? u0 + 0.25f * (u - u0) : u0 + (2.0f / 3.0f) * (u - u0);
 }
 
-template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB>
+// Whether work item w's input box lies inside its member's arrays (and the
+// member has tensor maps): then it is loaded by TMA.
+template <int TX, int TY, int BW, int BH>
+__device__ __forceinline__ bool tma_tile(const StageArgs& a, int w) {
+  const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
+  const Member& g = a.members[m];
+  if (!g.tmap) return false;
+  const int lt = w - g.tile_begin;
+  const int i0 = (lt % g.tiles_x) * TX, j0 = (lt / g.tiles_x) * TY;
+  return i0 >= 4 && i0 - 4 + BW <= g.nx && j0 >= 3 && j0 - 3 + BH <= g.ny;
+}
+
+// Thread 0: issue the six box loads of work item w's stage input.
+template <int STAGE, int TX, int TY, int BW, int BH, int BOXF>
+__device__ __forceinline__ void tma_issue(const StageArgs& a, int w, float* stg, uint64_t* bar) {
+  const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
+  const Member& g = a.members[m];
+  const int lt = w - g.tile_begin;
+  const int i0 = (lt % g.tiles_x) * TX, j0 = (lt / g.tiles_x) * TY;
+  const int sbuf = a.ctl[m].parity;
+  const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? 1 - sbuf : 2);
+  const char* maps = reinterpret_cast<const char*>(g.tmap) + size_t(in_buf) * 6 * TMAP_BYTES;
+  mbar_arrive_expect_tx(bar, unsigned(6 * BW * BH * sizeof(float)));
+#pragma unroll
+  for (int q = 0; q < 6; ++q) tma_load_2d(stg + q * BOXF, maps + q * TMAP_BYTES, i0 - 4, j0 - 3, bar);
+}
+
+template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB, bool TMA>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   using G = TileGeom32<TX, TY, SB>;
+  static_assert(!TMA || G::TMA_FITS, "TMA staging must fit in the slope arrays");
   using R = float;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);       // [6][NP]   primitives, tile + 2 halo
@@ -53,17 +96,48 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   R* sBy = sBx + G::NBX;
   __shared__ double red[NT / 32];
   __shared__ int s_last;
+  __shared__ __align__(8) uint64_t s_bar;    // TMA completion
+  // TMA pipeline state, kept in shared memory rather than in a register that
+  // would stay live through the register-bound flux phase: bit 0 = this tile's
+  // inputs come by TMA, bit 1 = the barrier parity to wait for.  Thread 0
+  // rewrites it only between barriers that every thread's reads precede.
+  __shared__ unsigned s_tma;
 
   const int tid = threadIdx.x;
   const bool slope_on = a.slope_limiting != 0;
   const bool mood_on = a.mood != 0;
   const bool van_leer = a.limiter == LIMITER_VAN_LEER;
+  // TMA staging area in the slope arrays, 128-byte aligned (recomputed where used)
+  auto staging = [&]() {
+    return reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sS + G::STG0) + 127) & ~uintptr_t(127));
+  };
+  constexpr unsigned TMA_POLLS = 1u << 26;   // bound of every wait for a TMA completion
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init(&s_bar, 1);
+      const bool st = blockIdx.x < unsigned(a.total_tiles) && tma_tile<TX, TY, G::BW, G::BH>(a, blockIdx.x);
+      s_tma = st ? 1u : 0u;
+      if (st) tma_issue<STAGE, TX, TY, G::BW, G::BH, G::BOXF>(a, blockIdx.x, staging(), &s_bar);
+    }
+    __syncthreads();
+  }
 
   for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
     const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
     const Member& g = a.members[m];
     Control* ctl = a.ctl + m;
-    if (ctl->active == 0) continue;
+    if (ctl->active == 0) {
+      if (TMA && (s_tma & 1u)) {   // a copy was issued for this tile: consume it to keep the phases paired
+        const bool ok = mbar_wait(&s_bar, (s_tma >> 1) & 1u, TMA_POLLS);
+        if (__syncthreads_or(!ok)) {   // a copy that never lands sets the status word and ends the kernel
+          if (tid == 0) atomicOr(&ctl->status, STATUS_TIMEOUT);
+          return;
+        }
+        if (tid == 0) s_tma = (s_tma ^ 2u) & ~1u;
+        __syncthreads();
+      }
+      continue;
+    }
     const int nx = g.nx, ny = g.ny;
     const int px = g.periodic_x, py = g.periodic_y;
     const int lt = w - g.tile_begin;
@@ -84,10 +158,35 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       u0[q] = reinterpret_cast<const R*>(g.buf[sbuf][q]);
       out[q] = reinterpret_cast<R*>(g.buf[out_buf][q]);
     }
-    prefetch_next_tile<R, TX, TY, NT, STAGE>(a, w + gridDim.x);
+    {
+      const int wn = w + gridDim.x;   // the next tile's inputs are prefetched to L2 unless TMA loads them
+      prefetch_next_tile<R, TX, TY, NT, STAGE>(
+          a, wn, !(TMA && wn < a.total_tiles && tma_tile<TX, TY, G::BW, G::BH>(a, wn)));
+    }
 
     // ---- phase 1: primitives (FP64 pressure recovery) -------------------------
-    {
+    bool tma_bad = false;
+    if (TMA && (s_tma & 1u)) {
+      // from the TMA box: element (x, y) of the box is cell (i0-4+x, j0-3+y); the
+      // box lies inside the arrays, so both face-B averages apply
+      const float* stg = staging();
+      tma_bad = !mbar_wait(&s_bar, (s_tma >> 1) & 1u, TMA_POLLS);
+      for (int p = tid; p < G::NP && !tma_bad; p += NT) {
+        const int qx = p % G::PX, qy = p / G::PX;
+        const int b = (qy + 1) * G::BW + (qx + 2);
+        const R Bx = R(0.5) * (stg[4 * G::BOXF + b] + stg[4 * G::BOXF + b - 1]);
+        const R By = R(0.5) * (stg[5 * G::BOXF + b] + stg[5 * G::BOXF + b - G::BW]);
+        const Prim<R> pr = get_primitive_mixed(stg[b], stg[G::BOXF + b], stg[2 * G::BOXF + b],
+                                               stg[3 * G::BOXF + b], Bx, By, g.gamma, g.inv_vol,
+                                               float(g.inv_vol));
+        sP[0 * G::NP + p] = pr.rho;
+        sP[1 * G::NP + p] = pr.vx;
+        sP[2 * G::NP + p] = pr.vy;
+        sP[3 * G::NP + p] = pr.P;
+        sP[4 * G::NP + p] = pr.Bx;
+        sP[5 * G::NP + p] = pr.By;
+      }
+    } else {
       // all of this thread's loads are issued before any arithmetic (memory-level parallelism)
       constexpr int KP = (G::NP + NT - 1) / NT;
       R ld[KP][8];
@@ -129,7 +228,15 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         }
       }
     }
-    __syncthreads();
+    if constexpr (TMA) {
+      if (__syncthreads_or(tma_bad)) {   // a copy that never lands sets the status word and ends the kernel
+        if (tid == 0) atomicOr(&ctl->status, STATUS_TIMEOUT);
+        return;
+      }
+    } else {
+      __syncthreads();
+    }
+
 
     // ---- phase 1.5: per-cell slopes and MOOD bounds -----------------------------
     // apply_slope_limiter (src/mhd_derivatives.f90:50-127) or compute_gradients
@@ -237,6 +344,20 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       if ((tid & 31) == 0 && s) atomicAdd(&ctl->mood_resets, (unsigned long long)s);
     }
     __syncthreads();
+    // the slopes are dead: the next tile's inputs stream in during phases 3a / 3b
+    if constexpr (TMA) {
+      if (tid == 0) {
+        const unsigned st = s_tma;     // this tile's state (every thread read it before phase 1's barrier)
+        const unsigned parity = ((st >> 1) ^ st) & 1u;   // flips if this tile consumed a completion
+        const int wn = w + gridDim.x;
+        const bool next = wn < a.total_tiles && tma_tile<TX, TY, G::BW, G::BH>(a, wn);
+        s_tma = (next ? 1u : 0u) | (parity << 1);
+        if (next) {
+          fence_proxy_async_smem();
+          tma_issue<STAGE, TX, TY, G::BW, G::BH, G::BOXF>(a, wn, staging(), &s_bar);
+        }
+      }
+    }
 
     // ---- phase 3a: constrained transport -> new face B ----------------------------
     const R* FByX = sFx + 4 * G::NFX;

@@ -126,3 +126,37 @@ def test_fp32_ensemble_error_is_the_conditioning_floor(G):
     floor = _ens_l1(runs["rounded"][1], runs["ref"][1])
     err = _ens_l1(runs["fp32"][1], runs["ref"][1])
     assert np.all(err <= 2.0 * floor + 1e-7), (err, floor)
+
+
+# (plain-load variant, TMA variant) pairs of the same tile shape and block size
+_TMA_PAIRS = [(5, 9), (6, 10)]
+
+
+@pytest.mark.parametrize("case", ["grf_ensemble", "rotor256", "ragged70"])
+def test_fp32_tma_variants_match_plain_loads(G, case):
+    """The TMA variants load interior tiles' inputs with box copies (edge tiles
+    and shapes without tensor maps use plain loads); they must reproduce the
+    plain-load variant of the same tile bit for bit."""
+    if case == "grf_ensemble":
+        cfgs, states = ensemble.grf_ensemble(16, FP32_BULK)
+    elif case == "rotor256":
+        cfg, st = P.rotor(256)
+        cfgs, states = [cfg.replace(precision=FP32_BULK)], [st]
+    else:   # nx not a multiple of 4: no tensor maps, every tile takes the plain path
+        cfg, st = P.orszag_tang(70)
+        cfgs, states = [cfg.replace(precision=FP32_BULK)], [st]
+    s = ensemble.make_batch(cfgs, states)
+    for plain, tma in _TMA_PAIRS:
+        outs = []
+        for v in (plain, tma):
+            for m, st in enumerate(states):
+                s.set_state(st, member=m)
+                s.set_time(0.0, 1, member=m)
+            s.set_variant(v)
+            s.step(12)
+            outs.append([s.get_state(member=m) for m in range(len(cfgs))])
+            assert s.diag()["status"] == 0
+        for a, b in zip(*outs):
+            for q in range(6):
+                assert np.array_equal(a[q], b[q]), (case, plain, tma, q)
+    s.close()
