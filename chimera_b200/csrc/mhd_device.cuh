@@ -24,9 +24,16 @@ template <typename R> struct K {
   static constexpr R e_floor_frac = R(1.0e-10);
 };
 
+// max / min / abs as the Fortran intrinsics evaluate them on finite values.
+// FP64 keeps the compare-and-select form (bit parity, signed zeros included);
+// the FP32-bulk form uses the single-instruction min / max / abs, which give
+// the same result on every finite input up to the sign of a zero result.
 template <typename R> __device__ __forceinline__ R dmax(R a, R b) { return (a > b) ? a : b; }
 template <typename R> __device__ __forceinline__ R dmin(R a, R b) { return (a < b) ? a : b; }
 template <typename R> __device__ __forceinline__ R dabs(R a) { return a < R(0) ? -a : a; }
+template <> __device__ __forceinline__ float dmax<float>(float a, float b) { return fmaxf(a, b); }
+template <> __device__ __forceinline__ float dmin<float>(float a, float b) { return fminf(a, b); }
+template <> __device__ __forceinline__ float dabs<float>(float a) { return fabsf(a); }
 __device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
 __device__ __forceinline__ double dcopysign(double a, double b) { return copysign(a, b); }

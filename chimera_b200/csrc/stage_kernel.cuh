@@ -69,27 +69,35 @@ __device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_nex
   const int i0 = (lt % g.tiles_x) * TX, j0 = (lt / g.tiles_x) * TY;
   const int sbuf = ctl->parity, obuf = 1 - sbuf;
   const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
-  const int c0 = max(i0 - 3, 0), c1 = min(i0 + TX + 2, nx) - 1;
   constexpr int LPR = ((TX + 5) * int(sizeof(R)) + 127) / 128 + 1;   // 128-B lines per row
-  constexpr int ROWS = TY + 5;
-  constexpr int ITEMS = 6 * ROWS * LPR;
-  constexpr int ITEMS0 = (STAGE >= 2) ? 6 * (TY + 1) * LPR : 0;
-  for (int it = threadIdx.x + (inputs ? 0 : ITEMS); it < ITEMS + ITEMS0; it += NT) {
-    const bool u0 = it >= ITEMS;
-    const int k = u0 ? it - ITEMS : it;
-    const int rows = u0 ? TY + 1 : ROWS;
-    const int q = k / (rows * LPR);
-    const int rem = k - q * rows * LPR;
-    const int r = rem / LPR, l = rem - (rem / LPR) * LPR;
-    const int gj = map_index((u0 ? j0 - 1 : j0 - 3) + r, ny, g.periodic_y);
-    const char* row = reinterpret_cast<const char*>(g.buf[u0 ? sbuf : in_buf][q]) + size_t(gj) * nx * sizeof(R);
-    const char* a0 = row + size_t(u0 ? max(i0 - 1, 0) : c0) * sizeof(R);
-    const char* a1 = row + size_t(u0 ? min(i0 + TX, nx) - 1 : c1) * sizeof(R);
-    // line l of the segment; line 0 starts at a0 itself so no address precedes the row
+  // line l of the segment [a0, a1]; line 0 starts at a0 itself so no address precedes the row
+  auto touch = [](const char* a0, const char* a1, int l) {
     const char* pl = (l == 0) ? a0
                               : reinterpret_cast<const char*>((reinterpret_cast<uintptr_t>(a0) & ~uintptr_t(127)) +
                                                               size_t(l) * 128);
     if (pl <= a1) asm volatile("prefetch.global.L2 [%0];" ::"l"(pl));
+  };
+  if (inputs) {   // the stage input over [i0-3, i0+TX+2) x [j0-3, j0+TY+2)
+    constexpr int ROWS = TY + 5;
+    const int c0 = max(i0 - 3, 0), c1 = min(i0 + TX + 2, nx) - 1;
+    for (int it = threadIdx.x; it < 6 * ROWS * LPR; it += NT) {
+      const int q = it / (ROWS * LPR), rem = it % (ROWS * LPR);
+      const int r = rem / LPR, l = rem % LPR;
+      const char* row = reinterpret_cast<const char*>(g.buf[in_buf][q]) +
+                        size_t(map_index(j0 - 3 + r, ny, g.periodic_y)) * nx * sizeof(R);
+      touch(row + size_t(c0) * sizeof(R), row + size_t(c1) * sizeof(R), l);
+    }
+  }
+  if (STAGE >= 2) {   // U^n over the tile (+1 halo face)
+    constexpr int ROWS0 = TY + 1;
+    const int c0 = max(i0 - 1, 0), c1 = min(i0 + TX, nx) - 1;
+    for (int it = threadIdx.x; it < 6 * ROWS0 * LPR; it += NT) {
+      const int q = it / (ROWS0 * LPR), rem = it % (ROWS0 * LPR);
+      const int r = rem / LPR, l = rem % LPR;
+      const char* row = reinterpret_cast<const char*>(g.buf[sbuf][q]) +
+                        size_t(map_index(j0 - 1 + r, ny, g.periodic_y)) * nx * sizeof(R);
+      touch(row + size_t(c0) * sizeof(R), row + size_t(c1) * sizeof(R), l);
+    }
   }
 }
 
