@@ -329,15 +329,16 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         if (mood_on) {
           // MOOD bounds of the LOW cell (:190-216), applied to both states and
           // resetting both to the low cell's value (the reference's XR/YR rule).
-          R lo = dmin(dmin(dmin(dmin(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
-          const R hi = dmax(dmax(dmax(dmax(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
-          if (rp) lo = dmax(R(0.1e-8), lo);
+          // (the bounds only feed comparisons: hardware min / max)
+          R lo = hmin(hmin(hmin(hmin(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
+          const R hi = hmax(hmax(hmax(hmax(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
+          if (rp) lo = hmax(R(0.1e-8), lo);
           if (vL < lo || vL > hi) { vL = f0; reset = true; }
           if (vR < lo || vR > hi) { vR = f0; reset = true; }
         }
         if (rp) {                      // face floors (:223-227)
-          vL = dmax(vL, R(1.0e-8));
-          vR = dmax(vR, R(1.0e-8));
+          vL = hmax(vL, R(1.0e-8));
+          vR = hmax(vR, R(1.0e-8));
         }
         L[q] = vL; Rv[q] = vR;
       }
