@@ -33,3 +33,19 @@ def energy_mean(snap, gamma):
     e = snap["P"] / (gamma - 1.0) + 0.5 * snap["rho"] * (snap["Vx"] ** 2 + snap["Vy"] ** 2) + \
         0.5 * (snap["Bx"] ** 2 + snap["By"] ** 2)
     return float(e.mean())
+
+
+def mass_drift(snaps):
+    """Largest relative change of the total density over the snapshots
+    (tests/physics/test_physics.py:46-60)."""
+    m0 = snaps[0]["rho"].sum()
+    return max(abs(s["rho"].sum() - m0) / m0 for s in snaps)
+
+
+def field_loop_l1(snaps):
+    """Mean |B| change of the advected loop, relative to its mean strength
+    (tests/physics/test_physics.py:118-141)."""
+    B0 = np.sqrt(snaps[0]["Bx"] ** 2 + snaps[0]["By"] ** 2)
+    Bf = np.sqrt(snaps[-1]["Bx"] ** 2 + snaps[-1]["By"] ** 2)
+    mean_B0 = B0[B0 > 1e-8].mean() if (B0 > 1e-8).any() else 1.0
+    return np.mean(np.abs(Bf - B0)) / mean_B0

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from chimera_b200 import problems as P
-from tests.snapshots import energy_mean, oracle_snapshots
+from tests.snapshots import energy_mean, field_loop_l1, mass_drift, oracle_snapshots
 
 
 @pytest.fixture(scope="module")
@@ -37,18 +37,13 @@ def fl64(oracle):
     return _fl(oracle, 64)
 
 
-def _mass_drift(snaps):
-    m0 = snaps[0]["rho"].sum()
-    return max(abs(s["rho"].sum() - m0) / m0 for s in snaps)
-
-
 # tests/physics/test_physics.py:46-60
 def test_mass_conserved_ot(ot32):
-    assert _mass_drift(ot32[1]) < 1e-10
+    assert mass_drift(ot32[1]) < 1e-10
 
 
 def test_mass_conserved_field_loop(fl32):
-    assert _mass_drift(fl32[1]) < 1e-10
+    assert mass_drift(fl32[1]) < 1e-10
 
 
 # tests/physics/test_physics.py:66-84
@@ -101,14 +96,7 @@ def test_ot_energy_monotone_early(ot64):
 
 
 # tests/physics/test_physics.py:118-141
-def _fl_l1(snaps):
-    B0 = np.sqrt(snaps[0]["Bx"] ** 2 + snaps[0]["By"] ** 2)
-    Bf = np.sqrt(snaps[-1]["Bx"] ** 2 + snaps[-1]["By"] ** 2)
-    mean_B0 = B0[B0 > 1e-8].mean() if (B0 > 1e-8).any() else 1.0
-    return np.mean(np.abs(Bf - B0)) / mean_B0
-
-
 def test_field_loop_convergence(fl32, fl64):
-    e32, e64 = _fl_l1(fl32[1]), _fl_l1(fl64[1])
+    e32, e64 = field_loop_l1(fl32[1]), field_loop_l1(fl64[1])
     assert e64 < e32
     assert e32 / e64 >= 1.5
