@@ -69,16 +69,36 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(key):
-    """Per-launch DRAM bytes of a kernel from a committed ncu summary
-    (``profiles/*.md`` lines of the form ``traffic[<key>]: <bytes>``)."""
+def profile_value(kind, key):
+    """A per-kernel figure from a committed ncu summary: ``profiles/*.md``
+    lines of the form ``<kind>[<key>]: <number>`` (kind ``traffic``: DRAM
+    bytes per launch; kind ``instructions``: thread instructions per cell)."""
+    pat = re.compile(r"\s*" + re.escape(kind) + r"\[(.+?)\]:\s*([0-9.eE+]+)")
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(path) as f:
             for line in f:
-                m = re.match(r"\s*traffic\[(.+?)\]:\s*([0-9.eE+]+)", line)
+                m = pat.match(line)
                 if m and m.group(1) == key:
                     return float(m.group(2))
     return None
+
+
+def profile_traffic(key):
+    return profile_value("traffic", key)
+
+
+def issue_roofline(inst_per_cell, cells, launch_ms, sm_mhz, n_sms):
+    """The instruction-issue roofline of a compute-bound kernel: warp
+    instructions issued per second (the ncu instruction count per cell x cells
+    / 32, over the live launch time) against 4 warp instructions per clock per
+    SM (one per scheduler) at the SM clock sampled during the timed region."""
+    if inst_per_cell is None or not sm_mhz:
+        return None
+    achieved = inst_per_cell * cells / 32.0 / (launch_ms * 1e-3) / 1e9
+    peak = 4.0 * n_sms * sm_mhz * 1e6 / 1e9
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "G warp-instructions/s",
+            "frac": achieved / peak, "instructions_per_cell": inst_per_cell,
+            "peak_kind": f"4 per clock per SM x {n_sms} SMs at the sampled {sm_mhz:.0f} MHz"}
 
 
 class Clocks:
@@ -322,6 +342,7 @@ def run_chimera(args, world, rank, local):
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg[dom] * 1e-3) / 1e9
     traffic = profile_traffic(f"{args.precision}_hlle_{dom}_rotor{n}")
+    inst_per_cell = profile_value("instructions", f"{args.precision}_hlle_{dom}_rotor{n}")
 
     # --- end to end through the C-ABI with host buffers: every step copies the
     #     state in from pinned host memory, advances one step, copies it out.
@@ -375,7 +396,9 @@ def run_chimera(args, world, rank, local):
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "avg_launch_ms": avg[dom], "per_kernel_avg_ms": avg},
+                         "avg_launch_ms": avg[dom], "per_kernel_avg_ms": avg,
+                         "issue": issue_roofline(inst_per_cell, cells, avg[dom], ck.get("sm_mhz"),
+                                                 torch.cuda.get_device_properties(local).multi_processor_count)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": 3 * args.steps,
