@@ -33,8 +33,11 @@ namespace chimera {
 __device__ __forceinline__ int map_index(int g, int n, int periodic) {
   if (g >= 0 && g < n) return g;
   if (periodic) {
-    int r = g % n;
-    return r < 0 ? r + n : r;
+    // g mod n by whole periods: one step for every grid of at least a tile's
+    // width, a few for tiny ones -- no integer division on the common path
+    while (g < 0) g += n;
+    while (g >= n) g -= n;
+    return g;
   }
   return g < 0 ? 0 : n - 1;
 }
