@@ -103,6 +103,10 @@ struct chimera_handle {
   char* d_tmaps = nullptr;           // [TMA variant slot][member][buffer 3][field 6] tensor maps
   std::vector<int> tmap_slot;        // per variant: its slot in d_tmaps, -1 without TMA
   std::vector<unsigned char> tmap_ok;   // [slot][member]: the member's maps exist
+  cudaStream_t copy_stream = nullptr;   // chimera_step_host: device-to-host copies of finished bands
+  // chimera_step_host: stage-3 band b written.  Four bands: each extra
+  // device-to-host copy costs about 3 us, against the compute of one band
+  cudaEvent_t band_done[4] = {};
   double* d_stage64 = nullptr;       // FP64 staging for FP32-bulk set/get
   size_t max_cells = 0;
   std::vector<bool> dt_valid;        // per member: Control::dt matches the state
@@ -172,31 +176,32 @@ static void harvest_profile(chimera_handle* h) {
   h->timed.clear();
 }
 
-static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid);
+static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_begin, int w_end);
 
 // kind: 0 = CFL kernel, 1..3 = stage kernels
 static int launch(chimera_handle* h, const KernelEntry& k, int grid, int kind) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(h->stream, &cs);
-  if (!h->profiling || cs != cudaStreamCaptureStatusNone) return launch_raw(h, k, grid);
+  if (!h->profiling || cs != cudaStreamCaptureStatusNone) return launch_raw(h, k, grid, 0, -1);
   if (h->timed.size() > 4096) harvest_profile(h);
   cudaEvent_t a = take_event(h), b = take_event(h);
-  if (!a || !b) return launch_raw(h, k, grid);
+  if (!a || !b) return launch_raw(h, k, grid, 0, -1);
   cudaEventRecord(a, h->stream);
-  int rc = launch_raw(h, k, grid);
+  int rc = launch_raw(h, k, grid, 0, -1);
   cudaEventRecord(b, h->stream);
   h->timed.push_back({kind, a, b});
   return rc;
 }
 
-static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid) {
+static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_begin, int w_end) {
   StageArgs a;
   a.members = h->d_members;
   a.ctl = h->d_ctl;
   a.partials = h->d_part;
   a.tile_member = h->d_tile_member;
   a.n_members = h->n;
-  a.total_tiles = h->total_tiles;
+  a.total_tiles = (w_end < 0) ? h->total_tiles : w_end;
+  a.work_begin = w_begin;
   a.limiter = h->limiter;
   a.slope_limiting = h->slope;
   a.mood = h->mood;
@@ -515,6 +520,9 @@ void chimera_destroy(chimera_handle* h) {
   cudaFree(h->d_tile_member);
   cudaFree(h->d_stage64);
   cudaFree(h->d_tmaps);
+  for (auto e : h->band_done)
+    if (e) cudaEventDestroy(e);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   cudaGetLastError();
   delete h;
@@ -624,6 +632,77 @@ int chimera_get_stage_buffer(chimera_handle* h, int b, double* Mass, double* Mom
   if (b < 0 || b > 2) return CHIMERA_ERR_BAD_ARG;
   double* p[6] = {Mass, Momx, Momy, Energy, b_x, b_y};
   return get_buffer(h, 0, b, p, ld, where);
+}
+
+// One RK3 step of a single-grid FP64 handle on host arrays: the state comes
+// in from `in`, advances one step and goes out to `out` (which may alias
+// `in`).  Stage 3 runs in bands of tile rows and each band's rows go back to
+// the host on a second stream as soon as the band is written, so the
+// device-to-host copy overlaps the rest of stage 3.  Other handles take the
+// set_state / step / get_state sequence.
+int chimera_step_host(chimera_handle* h, const double* const* in, double* const* out, int ld) {
+  if (!h || !in || !out) return CHIMERA_ERR_BAD_ARG;
+  const void* pi[6] = {in[0], in[1], in[2], in[3], in[4], in[5]};
+  const void* po[6] = {out[0], out[1], out[2], out[3], out[4], out[5]};
+  int rc = check_io(h, 0, pi, ld, CHIMERA_HOST);
+  if (!rc) rc = check_io(h, 0, po, ld, CHIMERA_HOST);
+  if (rc) return rc;
+  if (h->n != 1 || h->precision != CHIMERA_FP64 || h->graph_steps_request > 0) {
+    rc = chimera_set_state(h, in[0], in[1], in[2], in[3], in[4], in[5], ld, CHIMERA_HOST);
+    if (!rc) rc = chimera_step(h, 1);
+    if (!rc) rc = chimera_get_state(h, out[0], out[1], out[2], out[3], out[4], out[5], ld, CHIMERA_HOST);
+    return rc;
+  }
+  Control c;
+  rc = read_ctl(h, 0, &c);
+  if (rc) return rc;
+  const chimera_cfg& cf = h->cfg[0];
+  const Member& g = h->hm[0];
+  for (int q = 0; q < 6; ++q) {
+    rc = copy_field_in(h, 0, g.buf[c.parity][q], in[q], ld, CHIMERA_HOST);
+    if (rc) return rc;
+  }
+  h->dt_valid[0] = false;
+  if (!c.active) {   // t >= t_end: no step is taken, the state goes back unchanged
+    for (int q = 0; q < 6; ++q) {
+      rc = copy_field_out(h, 0, out[q], g.buf[c.parity][q], ld, CHIMERA_HOST);
+      if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return CHIMERA_OK;
+  }
+  rc = ensure_dt(h);
+  for (int s = 0; s < 2 && !rc; ++s) rc = launch(h, h->ks.stage[h->riemann - 1][s], h->grid_stage[s], s + 1);
+  if (rc) return rc;
+  if (!h->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    for (auto& e : h->band_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // bands of tile rows (work items are row-major within the grid)
+  const int ty = h->ks.stage[0][0].ty;
+  const int rows = g.tiles_y, nb = std::min(rows, int(sizeof(h->band_done) / sizeof(h->band_done[0])));
+  const int out_buf = 1 - c.parity;   // stage 3 writes U^{n+1} there; the finish flips the parity
+  const KernelEntry& k3 = h->ks.stage[h->riemann - 1][2];
+  for (int b = 0; b < nb; ++b) {
+    const int r0 = rows * b / nb, r1 = rows * (b + 1) / nb;
+    const int w0 = r0 * g.tiles_x, w1 = r1 * g.tiles_x;
+    const int grid = std::max(1, std::min(h->grid_stage[2], w1 - w0));
+    rc = launch_raw(h, k3, grid, w0, w1);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->band_done[b], h->stream));
+    CK(cudaStreamWaitEvent(h->copy_stream, h->band_done[b], 0));
+    const int y0 = r0 * ty, y1 = std::min(r1 * ty, cf.ny);
+    const size_t w = size_t(cf.nx) * sizeof(double);
+    for (int q = 0; q < 6; ++q)
+      CK(cudaMemcpy2DAsync(out[q] + size_t(y0) * ld, size_t(ld) * sizeof(double),
+                           static_cast<const char*>(g.buf[out_buf][q]) + size_t(y0) * w, w, w, y1 - y0,
+                           cudaMemcpyDeviceToHost, h->copy_stream));
+  }
+  h->dt_valid[0] = true;   // the stage-3 finish computed the next dt
+  CK(cudaStreamSynchronize(h->copy_stream));
+  rc = read_ctl(h, 0, &c);
+  if (rc) return rc;
+  return c.status ? CHIMERA_ERR_NONFINITE : CHIMERA_OK;
 }
 
 int chimera_batch_set_time(chimera_handle* h, int m, double t, int output_count) {

@@ -52,7 +52,8 @@ struct StageArgs {
   double* partials;        // [total_tiles][NPART]
   const int* tile_member;  // work index -> member (n_members > 1)
   int n_members;
-  int total_tiles;
+  int total_tiles;          // one past the last work item of this launch
+  int work_begin;           // first work item of this launch (0 unless a launch covers a band of rows)
   int limiter, slope_limiting, mood;
   int counters;            // count MOOD resets / floor hits
   int dry;                 // timing run: write scratch only, leave Control untouched

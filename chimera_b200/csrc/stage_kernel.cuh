@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   const bool mood_on = a.mood != 0;
   const bool van_leer = a.limiter == LIMITER_VAN_LEER;
 
-  for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
+  for (int w = a.work_begin + blockIdx.x; w < a.total_tiles; w += gridDim.x) {
     const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
     const Member& g = a.members[m];
     Control* ctl = a.ctl + m;
@@ -549,7 +549,7 @@ template <typename R, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
   __shared__ double red[NT / 32];
   __shared__ int s_last;
-  for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
+  for (int w = a.work_begin + blockIdx.x; w < a.total_tiles; w += gridDim.x) {
     const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
     const Member& g = a.members[m];
     Control* ctl = a.ctl + m;

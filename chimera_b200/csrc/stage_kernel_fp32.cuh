@@ -115,14 +115,15 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   if constexpr (TMA) {
     if (tid == 0) {
       mbar_init(&s_bar, 1);
-      const bool st = blockIdx.x < unsigned(a.total_tiles) && tma_tile<TX, TY, G::BW, G::BH>(a, blockIdx.x);
+      const int w0 = a.work_begin + int(blockIdx.x);
+      const bool st = w0 < a.total_tiles && tma_tile<TX, TY, G::BW, G::BH>(a, w0);
       s_tma = st ? 1u : 0u;
-      if (st) tma_issue<STAGE, TX, TY, G::BW, G::BH, G::BOXF>(a, blockIdx.x, staging(), &s_bar);
+      if (st) tma_issue<STAGE, TX, TY, G::BW, G::BH, G::BOXF>(a, w0, staging(), &s_bar);
     }
     __syncthreads();
   }
 
-  for (int w = blockIdx.x; w < a.total_tiles; w += gridDim.x) {
+  for (int w = a.work_begin + blockIdx.x; w < a.total_tiles; w += gridDim.x) {
     const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
     const Member& g = a.members[m];
     Control* ctl = a.ctl + m;

@@ -82,6 +82,7 @@ def lib():
         L.chimera_get_stage_buffer.argtypes = io
         L.chimera_batch_set_time.argtypes = [P, C.c_int, C.c_double, C.c_int]
         L.chimera_step.argtypes = [P, C.c_int]
+        L.chimera_step_host.argtypes = [P, P * 6, P * 6, C.c_int]
         L.chimera_advance.argtypes = [P, C.c_int, C.POINTER(C.c_int)]
         L.chimera_stage.argtypes = [P, C.c_int, C.c_double]
         L.chimera_batch_diag.argtypes = [P, C.c_int, C.POINTER(CDiag)]
@@ -205,6 +206,22 @@ class Solver:
 
     def step(self, nsteps: int = 1):
         _check(lib().chimera_step(self._h, int(nsteps)), "step")
+
+    def step_host(self, inputs: Sequence, out=None):
+        """One step on host arrays (chimera_step_host): ``inputs`` (six numpy
+        arrays or CPU tensors, pinned for copy overlap) in, the new state to
+        ``out`` (default: new numpy arrays; may be ``inputs``)."""
+        c = self.cfgs[0]
+        if out is None:
+            out = [np.empty((c.ny, c.nx), dtype=np.float64) for _ in range(6)]
+        pi, ld_i, wi, keep_i = _ptrs(inputs, c.nx, c.ny)
+        po, ld_o, wo, keep_o = _ptrs(out, c.nx, c.ny)
+        if wi != HOST or wo != HOST or ld_i != ld_o:
+            raise ValueError("step_host takes host arrays with one pitch")
+        P6 = C.c_void_p * 6
+        _check(lib().chimera_step_host(self._h, P6(*[p.value for p in pi]), P6(*[p.value for p in po]), ld_i),
+               "step_host")
+        return out
 
     def advance(self, max_steps: int = 10 ** 9) -> int:
         n = C.c_int(0)

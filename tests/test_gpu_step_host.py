@@ -1,0 +1,90 @@
+"""chimera_step_host: one step on host arrays, with the device-to-host copy of
+stage 3's finished row bands overlapping the rest of the stage.  It must give
+exactly what set_state + step + get_state give."""
+import numpy as np
+import pytest
+import torch
+
+from chimera_b200 import problems as P
+from chimera_b200.config import BC_OUTFLOW, BC_PERIODIC, FP32_BULK
+from tests.gpu_util import require_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def G():
+    return require_gpu()
+
+
+def _reference_steps(G, cfg, st, n):
+    s = G.Solver(cfg)
+    out, states = st, []
+    for _ in range(n):
+        s.set_state(out)
+        s.step(1)
+        out = s.get_state()
+        states.append((out, s.diag()))
+    s.close()
+    return states
+
+
+def _pinned(arrays):
+    return [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in arrays]
+
+
+@pytest.mark.parametrize("case", ["rotor128", "ragged50x37", "ot96"])
+def test_step_host_equals_set_step_get(G, case):
+    if case == "rotor128":
+        cfg, st = P.rotor(128)
+    elif case == "ragged50x37":
+        cfg, st = P.orszag_tang(50)
+        cfg = cfg.replace(bc=(BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW))
+        st = [a[:37].copy() for a in st]
+        cfg = cfg.replace(ny=37)
+    else:
+        cfg, st = P.orszag_tang(96)
+    ref = _reference_steps(G, cfg, st, 3)
+    s = G.Solver(cfg)
+    buf = _pinned(st)
+    for k in range(3):
+        s.step_host(buf, out=buf)                 # in place, pinned
+        for q in range(6):
+            assert np.array_equal(buf[q].numpy(), ref[k][0][q]), (k, q)
+        d = s.diag()
+        assert (d["t"], d["dt"], d["output_count"]) == (ref[k][1]["t"], ref[k][1]["dt"], ref[k][1]["output_count"])
+    s.close()
+
+
+def test_step_host_then_device_steps(G):
+    """After step_host the handle holds the new state and its dt: device steps continue from it."""
+    cfg, st = P.rotor(64)
+    a = G.Solver(cfg)
+    a.set_state(st)
+    a.step(3)
+    b = G.Solver(cfg)
+    b.step_host(st)
+    b.step(2)
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(x, y)
+
+
+def test_step_host_inactive_returns_input(G):
+    cfg, st = P.orszag_tang(32, t_end=0.5)
+    s = G.Solver(cfg)
+    s.set_time(0.6, 61)
+    out = s.step_host(st)
+    for x, y in zip(out, st):
+        assert np.array_equal(x, y)
+
+
+def test_step_host_fp32_handle(G):
+    cfg, st = P.orszag_tang(64)
+    c32 = cfg.replace(precision=FP32_BULK)
+    ref = _reference_steps(G, c32, st, 2)
+    s = G.Solver(c32)
+    out = st
+    for k in range(2):
+        out = s.step_host(out)
+        for q in range(6):
+            assert np.array_equal(out[q], ref[k][0][q])
