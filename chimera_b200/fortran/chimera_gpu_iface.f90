@@ -11,7 +11,7 @@ module chimera_gpu_iface
     private
     public :: chimera_cfg, chimera_diag_out
     public :: chimera_create, chimera_destroy, chimera_set_state, chimera_get_state
-    public :: chimera_set_time, chimera_step, chimera_advance, chimera_diag
+    public :: chimera_set_time, chimera_step, chimera_advance, chimera_diag, chimera_step_host
     public :: chimera_batch_create, chimera_batch_set_state, chimera_batch_get_state
     public :: chimera_batch_set_time, chimera_batch_diag, chimera_set_graph_steps
     public :: chimera_autotune, chimera_set_variant
@@ -82,6 +82,15 @@ module chimera_gpu_iface
             import :: c_int, c_ptr
             type(c_ptr), value :: h
             integer(c_int), value :: nsteps
+        end function
+
+        ! one step on host arrays: ptrs = [c_loc(Mass), c_loc(Momx), ..., c_loc(b_y)] of
+        ! target arrays (ld, ny); out_ptrs may equal in_ptrs
+        integer(c_int) function chimera_step_host(h, in_ptrs, out_ptrs, ld) bind(C, name="chimera_step_host")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr), intent(in) :: in_ptrs(6), out_ptrs(6)
+            integer(c_int), value :: ld
         end function
 
         integer(c_int) function chimera_advance(h, max_steps, steps_taken) bind(C, name="chimera_advance")
