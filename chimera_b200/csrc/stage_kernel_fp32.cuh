@@ -278,67 +278,78 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
     __syncthreads();
 
     // ---- phase 2: face fluxes ------------------------------------------------------
+    // One work item per low cell of the slope grid: its x face (i+1/2, j) and
+    // its y face (i, j+1/2), where the tile needs them, share the cell's MOOD
+    // bounds (the 5-point stencil of src/mhd_derivatives.f90:190-211), which
+    // are formed once (SB: loaded once).
     unsigned mood_resets = 0;
-    for (int f = tid; f < G::NFX + G::NFY; f += NT) {
-      const bool ydir = f >= G::NFX;
-      const int ff = ydir ? f - G::NFX : f;
-      const int li = ydir ? ff % G::FYW : ff % G::FXW;
-      const int lj = ydir ? ff / G::FYW : ff / G::FXW;
-      const int sa = lj * G::SX + li;                       // low cell in the slope grid
-      const int sb = sa + (ydir ? G::SX : 1);                // high cell
-      const int pa = (lj + 1) * G::PX + (li + 1);             // low cell in the primitive grid
-      const int pb = pa + (ydir ? G::PX : 1);
-      const R hh = R(ydir ? g.hy : g.hx);
-      const int d = ydir ? 1 : 0;
-      R L[6], Rv[6];
-      bool reset = false;
+    for (int c = tid; c < G::NS; c += NT) {
+      const int cx = c % G::SX, cy = c / G::SX;
+      const int pa = (cy + 1) * G::PX + (cx + 1);             // the low cell in the primitive grid
+      R lo[6], hi[6];
+      if (mood_on) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const R f0 = sP[q * G::NP + pa], fp = sP[q * G::NP + pb];
-        R vL = f0 + hh * sS[(2 * q + d) * G::NS + sa];
-        R vR = fp - hh * sS[(2 * q + d) * G::NS + sb];
-        if (mood_on) {   // bounds of the LOW cell, reset to its value (src/mhd_derivatives.f90:213-216)
-          R lo, hi;
+        for (int q = 0; q < 6; ++q) {
           if (SB) {
-            lo = sLo[q * G::NS + sa];
-            hi = sHi[q * G::NS + sa];
-          } else {       // the 5-point stencil of the low cell (:190-211), as phase 1.5 forms it
+            lo[q] = sLo[q * G::NS + c];
+            hi[q] = sHi[q * G::NS + c];
+          } else {
             const R* s = sP + q * G::NP;
-            const R xp = s[pa + 1], xm = s[pa - 1], yp = s[pa + G::PX], ym = s[pa - G::PX];
-            lo = fminf(fminf(fminf(fminf(f0, xp), xm), yp), ym);
-            hi = fmaxf(fmaxf(fmaxf(fmaxf(f0, xp), xm), yp), ym);
-            if (q == 0 || q == 3) lo = fmaxf(R(0.1e-8), lo);
+            const R f0 = s[pa], xp = s[pa + 1], xm = s[pa - 1], yp = s[pa + G::PX], ym = s[pa - G::PX];
+            R l = fminf(fminf(fminf(fminf(f0, xp), xm), yp), ym);
+            hi[q] = fmaxf(fmaxf(fmaxf(fmaxf(f0, xp), xm), yp), ym);
+            if (q == 0 || q == 3) l = fmaxf(R(0.1e-8), l);
+            lo[q] = l;
           }
-          if (vL < lo || vL > hi) { vL = f0; reset = true; }
-          if (vR < lo || vR > hi) { vR = f0; reset = true; }
         }
-        if (q == 0 || q == 3) {
-          vL = fmaxf(vL, R(1.0e-8));
-          vR = fmaxf(vR, R(1.0e-8));
+      }
+#pragma unroll 1
+      for (int d = 0; d < 2; ++d) {
+        const bool ydir = d == 1;
+        if (ydir ? (cy >= G::SY - 1) : (cx >= G::SX - 1)) continue;   // face outside the tile's set
+        const int ff = ydir ? cy * G::FYW + cx : cy * G::FXW + cx;
+        const int sb = c + (ydir ? G::SX : 1);                // high cell in the slope grid
+        const int pb = pa + (ydir ? G::PX : 1);
+        const R hh = R(ydir ? g.hy : g.hx);
+        R L[6], Rv[6];
+        bool reset = false;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const R f0 = sP[q * G::NP + pa], fp = sP[q * G::NP + pb];
+          R vL = f0 + hh * sS[(2 * q + d) * G::NS + c];
+          R vR = fp - hh * sS[(2 * q + d) * G::NS + sb];
+          if (mood_on) {   // bounds of the LOW cell, reset to its value (src/mhd_derivatives.f90:213-216)
+            if (vL < lo[q] || vL > hi[q]) { vL = f0; reset = true; }
+            if (vR < lo[q] || vR > hi[q]) { vR = f0; reset = true; }
+          }
+          if (q == 0 || q == 3) {
+            vL = fmaxf(vL, R(1.0e-8));
+            vR = fmaxf(vR, R(1.0e-8));
+          }
+          L[q] = vL; Rv[q] = vR;
         }
-        L[q] = vL; Rv[q] = vR;
-      }
-      if (L[3] - R(0.5) * (L[4] * L[4] + L[5] * L[5]) < K<R>::P_floor) {
+        if (L[3] - R(0.5) * (L[4] * L[4] + L[5] * L[5]) < K<R>::P_floor) {
 #pragma unroll
-        for (int q = 0; q < 6; ++q) L[q] = sP[q * G::NP + pa];
-      }
-      if (Rv[3] - R(0.5) * (Rv[4] * Rv[4] + Rv[5] * Rv[5]) < K<R>::P_floor) {
+          for (int q = 0; q < 6; ++q) L[q] = sP[q * G::NP + pa];
+        }
+        if (Rv[3] - R(0.5) * (Rv[4] * Rv[4] + Rv[5] * Rv[5]) < K<R>::P_floor) {
 #pragma unroll
-        for (int q = 0; q < 6; ++q) Rv[q] = sP[q * G::NP + pa];
+          for (int q = 0; q < 6; ++q) Rv[q] = sP[q * G::NP + pa];
+        }
+        mood_resets += reset ? 1u : 0u;
+        const R unL = ydir ? L[2] : L[1], unR = ydir ? Rv[2] : Rv[1];
+        const R utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
+        const R bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
+        const R btL = ydir ? L[4] : L[5], btR = ydir ? Rv[4] : Rv[5];
+        Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
+        R* dst = ydir ? sFy : sFx;
+        const int NF = ydir ? G::NFY : G::NFX;
+        dst[0 * NF + ff] = F.mass;
+        dst[1 * NF + ff] = ydir ? F.momt : F.momn;
+        dst[2 * NF + ff] = ydir ? F.momn : F.momt;
+        dst[3 * NF + ff] = F.energy;
+        dst[4 * NF + ff] = F.bt;
       }
-      mood_resets += reset ? 1u : 0u;
-      const R unL = ydir ? L[2] : L[1], unR = ydir ? Rv[2] : Rv[1];
-      const R utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
-      const R bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
-      const R btL = ydir ? L[4] : L[5], btR = ydir ? Rv[4] : Rv[5];
-      Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
-      R* dst = ydir ? sFy : sFx;
-      const int NF = ydir ? G::NFY : G::NFX;
-      dst[0 * NF + ff] = F.mass;
-      dst[1 * NF + ff] = ydir ? F.momt : F.momn;
-      dst[2 * NF + ff] = ydir ? F.momn : F.momt;
-      dst[3 * NF + ff] = F.energy;
-      dst[4 * NF + ff] = F.bt;
     }
     if (a.counters && !a.dry) {
       unsigned s = __reduce_add_sync(0xffffffffu, mood_resets);
