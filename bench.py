@@ -55,6 +55,12 @@ def parse():
                    help="force a tile variant for the FP32-batched ensemble (-1: autotune)")
     p.add_argument("--ens-forms", default="fp32,fp64",
                    help="ensemble forms to measure (the L1 comparison needs both)")
+    p.add_argument("--kh", choices=("on", "off"), default="on",
+                   help="also measure the Kelvin-Helmholtz HLLD comparison (FP32-bulk vs FP64)")
+    p.add_argument("--kh-n", type=int, default=4096)
+    p.add_argument("--kh-steps", type=int, default=1000)
+    p.add_argument("--adjoint", choices=("on", "off"), default="on",
+                   help="also measure the field-loop adjoint (forward + backward, central differences)")
     p.add_argument("--variant", type=int, default=-1,
                    help="force a tile variant for the single-grid measurement (-1: autotune)")
     return p.parse_args()
@@ -371,6 +377,12 @@ def run_chimera(args, world, rank, local):
                "steps": k2, "mode": "state copied host->device and back around every RK3 step "
                        "(chimera_step_host: stage 3's finished row bands go back while later bands compute)"}
 
+    kh = adj_leg = None
+    if world == 1 and args.kh == "on":
+        kh = run_kh(args)
+    if world == 1 and args.adjoint == "on":
+        adj_leg = run_adjoint_leg(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, done, el = cpu_reference_rate(n, 4, max_seconds=20.0)
@@ -407,6 +419,8 @@ def run_chimera(args, world, rank, local):
             "gpu_launches": 3 * args.steps,
             "clocks": ck,
             "forms": ens,
+            "kelvin_helmholtz": kh,
+            "adjoint": adj_leg,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -511,6 +525,132 @@ def run_ensemble(args, world):
     res["workload"] = (f"GRF ensemble, {res['fp32_batched']['members']} members of uneven sizes "
                        f"(128^2/256^2/512^2), periodic, Rusanov + MC + MOOD, {steps} RK3 steps")
     return res
+
+
+def _timed_run(s, steps, graph):
+    """Device time (ms) of `steps` steps on the solver's stream, replayed
+    from a graph of `graph` steps (captured by the caller beforehand)."""
+    import torch
+    ext = torch.cuda.ExternalStream(s.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(ext)
+    for _ in range(steps // graph):
+        s.step(graph)
+    e1.record(ext)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_kh(args):
+    """Kelvin-Helmholtz n^2 on [0,1]x[-1,1] (HLLD + MC + MOOD), the FP32-bulk
+    form against the plain FP64 form on the same GPU from the same state:
+    zone-cycles/s of each (graph replay), L1 error per field and div B."""
+    import numpy as np
+    from chimera_b200 import gpu, problems
+    from chimera_b200.config import FP32_BULK, FP64
+    n, steps = args.kh_n, args.kh_steps
+    graph = 10 if steps % 10 == 0 else 1
+    cfg, st = problems.kelvin_helmholtz(n)
+    res, finals = {}, {}
+    for name, prec in (("fp32_bulk", FP32_BULK), ("fp64", FP64)):
+        s = gpu.Solver(cfg.replace(precision=prec))
+        s.set_state(st)
+        s.autotune(reps=1)
+        s.set_graph_steps(graph)
+        s.step(graph)                                   # capture (not timed)
+        s.set_state(st)
+        s.set_time(0.0, 1)
+        s.step(0)
+        ms = _timed_run(s, steps, graph)
+        d = s.diag()
+        finals[name] = s.get_state()
+        res[name] = {"value": n * n * steps / (ms * 1e-3), "unit": "zone-cycles/s", "ms": ms,
+                     "divb_rel": d["divb_rel"], "tile": s.variant()}
+        s.close()
+    l1 = {}
+    for q, f in enumerate(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y")):
+        a, b = finals["fp32_bulk"][q], finals["fp64"][q]
+        l1[f] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+    res["fp32_l1_vs_fp64"] = l1
+    res["fp32_over_fp64"] = res["fp32_bulk"]["value"] / res["fp64"]["value"]
+    res["workload"] = (f"Kelvin-Helmholtz {n}^2 on [0,1]x[-1,1], periodic, HLLD + MC + MOOD, gamma 1.4, "
+                       f"{steps} RK3 steps from the same state")
+    return res
+
+
+def run_adjoint_leg(args):
+    """The field-loop adjoint (512^2 on [0,2]x[0,1], v = (2, 1), HLLE + Van
+    Leer, 400 RK3 steps, checkpoints every 20, loss = final magnetic energy,
+    gradient w.r.t. the initial rho, vx, vy): forward and forward + backward
+    times, and central differences on two smooth random directions."""
+    import time
+    import numpy as np
+    import torch
+    from chimera_b200 import adjoint, problems
+    from chimera_b200.config import HLLE, VAN_LEER
+    n, steps, K = 512, 400, 20
+    cfg, st = problems.field_loop(n, n, 2.0, 1.0, v=(2.0, 1.0), riemann=HLLE, limiter=VAN_LEER)
+    vol = cfg.dx * cfg.dy
+    M, Mx, My, E, bx, by = st
+    Bx, By = problems.face_to_cell(bx, by)
+    rho, vx, vy = M / vol, Mx / M, My / M
+    p = (E / vol - 0.5 * rho * (vx * vx + vy * vy) - 0.5 * (Bx * Bx + By * By)) * (cfg.gamma - 1.0)
+    prims = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (rho, vx, vy, p, bx, by)]
+    U0 = [u.contiguous() for u in adjoint.conserved_from_primitive(cfg, *prims)]
+    dts = adjoint.cfl_dts(cfg, U0, steps)
+    adj = adjoint.Adjoint(cfg)
+
+    def loss_of(pr, grad):
+        U = [u.contiguous() for u in adjoint.conserved_from_primitive(cfg, *pr)]
+        if not grad:
+            for dt in dts:
+                U = adj.forward_step(U, dt)
+            return adjoint.magnetic_energy(cfg, U)
+        return adjoint.magnetic_energy(cfg, adjoint.run(adj, U, dts, K=K))
+
+    with torch.no_grad():
+        loss_of(prims, False)                           # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.no_grad():
+        base = float(loss_of(prims, False))
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    g_in = [x.clone().requires_grad_(k < 3) for k, x in enumerate(prims)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = loss_of(g_in, True)
+    loss.backward()
+    torch.cuda.synchronize()
+    t_fb = time.perf_counter() - t0
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    kx = 2 * np.pi * torch.fft.fftfreq(n, d=cfg.dx, device="cuda", dtype=torch.float64)
+    ky = 2 * np.pi * torch.fft.fftfreq(n, d=cfg.dy, device="cuda", dtype=torch.float64)
+    filt = torch.exp(-0.5 * 0.25 ** 2 * (ky[:, None] ** 2 + kx[None, :] ** 2))
+    worst = 0.0
+    for _ in range(2):
+        dirs = []
+        for k in range(3):
+            w = torch.fft.ifft2(torch.fft.fft2(torch.randn((n, n), generator=gen, device="cuda",
+                                                           dtype=torch.float64)) * filt).real
+            dirs.append(w / torch.max(torch.abs(w)) * (float(torch.max(torch.abs(prims[k]))) or 1.0))
+        eps = 1e-6
+        with torch.no_grad():
+            lp = float(loss_of([prims[k] + eps * dirs[k] if k < 3 else prims[k] for k in range(6)], False))
+            lm = float(loss_of([prims[k] - eps * dirs[k] if k < 3 else prims[k] for k in range(6)], False))
+        fd = (lp - lm) / (2 * eps)
+        an = sum(float(torch.sum(g_in[k].grad * dirs[k])) for k in range(3))
+        worst = max(worst, abs(fd - an) / abs(an))
+    return {"workload": "field-loop adjoint 512^2 on [0,2]x[0,1], v = (2, 1), HLLE + Van Leer, 400 RK3 steps, "
+                        "K = 20, loss = final magnetic energy, gradient w.r.t. initial rho, vx, vy",
+            "forward_s": t_fwd, "forward_backward_s": t_fb, "loss": base,
+            "gradient_zone_cycles_per_s": n * n * steps / t_fb,
+            "central_difference_rel_err_2_dirs": worst,
+            "note": "rho and v start exactly uniform, so every rho / v limiter starts at its kink: central "
+                    "differences agree with the stated one-sided convention to about 3e-3 here, and to 1e-6 "
+                    "on a generic state (tests/test_gpu_adjoint.py)"}
 
 
 def main():
