@@ -76,6 +76,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
     os.replace(LIB + ".tmp", LIB)
+    # objects of earlier source versions are never linked again: drop them
+    current = {os.path.basename(o) for o in objs}
+    for name in os.listdir(BUILD):
+        if name.endswith(".o") and name not in current:
+            os.remove(os.path.join(BUILD, name))
     return LIB
 
 

@@ -3,9 +3,11 @@
 // Same stage operator and tile structure as stage_kernel (stage_kernel.cuh),
 // with the freedom the FP32 form has (it is checked against the FP64 oracle in
 // L1, not bit for bit) spent on fewer instructions per cell:
-//   * phase 1.5 computes each cell's limited x and y slopes and MOOD bounds
-//     once into shared memory; the FP64 kernel recomputes them for each face
-//     that touches the cell (twice per direction);
+//   * phase 1.5 computes each cell's limited x and y slopes once into shared
+//     memory (the FP64 kernel recomputes them for each face that touches the
+//     cell, twice per direction), and the MOOD bounds either there too (SB)
+//     or in phase 2, once per low cell for its x and y faces;
+//   * FP32 min / max / abs are the single hardware instructions;
 //   * the translation unit is compiled with fast FP32 division and square
 //     root (-use_fast_math), about 1 ulp instead of correctly rounded;
 //   * (TMA variants) the inputs of the CTA's next tile are loaded by TMA box
@@ -23,8 +25,8 @@
 
 namespace chimera {
 
-// Shared-memory plan.  SB: MOOD bounds stored per cell (12 arrays) or
-// recomputed per face from the primitives.  The new face-B arrays of phase 3a
+// Shared-memory plan.  SB: MOOD bounds stored per cell (12 arrays) or formed
+// in phase 2 from the primitives.  The new face-B arrays of phase 3a
 // reuse the slope arrays, which are dead once the face fluxes exist.
 // TMA staging: the six input fields over the box [i0-4, i0-4+BW) x [j0-3,
 // j0-3+BH) -- the primitives' 2-cell halo plus b_x(i-1), b_y(j-1) -- with the
