@@ -124,14 +124,6 @@ __device__ __forceinline__ R limit_slope(R dfL, R dfR) {
   return dcopysign(R(1), dfL) * hmin(hmin(R(2) * habs(dfL), R(2) * habs(dfR)), R(0.5) * habs(den));
 }
 
-// Slope of cell c from its two neighbours: the limiter (useSlopeLimiting) or
-// the central difference of compute_gradients (src/mhd_derivatives.f90:44-45).
-template <typename R, int LIMITER, bool SLOPE>
-__device__ __forceinline__ R cell_slope(R fm, R f0, R fp, R inv_h, R inv_2h) {
-  if (SLOPE) return limit_slope<R, LIMITER>((f0 - fm) * inv_h, (fp - f0) * inv_h);
-  return (fp - fm) * inv_2h;
-}
-
 // One face's 5 fluxes in (normal, tangential) orientation.
 template <typename R> struct Flux5 {
   R mass, momn, momt, energy, bt;
