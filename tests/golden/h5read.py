@@ -12,7 +12,6 @@ imports it.
 """
 from __future__ import annotations
 
-import struct
 import zlib
 
 import numpy as np
@@ -77,8 +76,7 @@ class _File:
         while stack:
             node = stack.pop()
             sig = self.b[node:node + 4]
-            if sig == b"TREE":
-                level = self.b[node + 5]
+            if sig == b"TREE":         # internal or leaf node: its children are nodes or SNODs
                 used = self.u(node + 6, 2)
                 p = node + 8 + 16          # after left / right sibling addresses
                 p += 8                     # key 0
@@ -86,7 +84,6 @@ class _File:
                     child = self.u(p, 8)
                     p += 16                # child address, next key
                     stack.append(child)
-                del level
             elif sig == b"SNOD":
                 n = self.u(node + 6, 2)
                 for k in range(n):

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from chimera_b200 import problems as P
-from chimera_b200.config import BC_OUTFLOW, BC_PERIODIC, FP32_BULK, HLLE, RUSANOV
+from chimera_b200.config import BC_OUTFLOW, FP32_BULK
 from tests.gpu_util import require_gpu
 
 pytestmark = pytest.mark.gpu

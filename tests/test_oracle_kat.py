@@ -2,7 +2,6 @@
 
 Each test cites the Fortran test it restates; tolerances are the reference's.
 """
-import math
 
 import numpy as np
 import pytest

@@ -6,7 +6,7 @@ import pytest
 import torch
 
 from chimera_b200 import problems as P
-from chimera_b200.config import HLLD, HLLE, MC, RUSANOV, VAN_LEER, BC_OUTFLOW, BC_PERIODIC
+from chimera_b200.config import HLLD, HLLE, VAN_LEER, BC_OUTFLOW, BC_PERIODIC
 from oracle import torch_ref as T
 
 CASES = {

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from chimera_b200 import problems as P
-from chimera_b200.config import BC_OUTFLOW, HLLD, HLLE, RUSANOV
+from chimera_b200.config import HLLD, HLLE, RUSANOV
 from tests.gpu_util import require_gpu
 
 pytestmark = pytest.mark.gpu
