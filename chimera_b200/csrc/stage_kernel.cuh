@@ -414,7 +414,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         val = in[4][idx] + dt * dbx;
         if (STAGE == 2) val = R(0.75) * u0[4][idx] + R(0.25) * val;
         if (STAGE == 3) val = R(1.0 / 3.0) * u0[4][idx] + R(2.0 / 3.0) * val;
-        sBx[lj * G::BXW + (li + 1)] = val;
+        if (STAGE == 3) sBx[lj * G::BXW + (li + 1)] = val;   // the epilogue reads neighbours' new B
+        else out[4][idx] = val;                                // stages 1, 2: straight to the output
       } else {
         const R e0 = Ez(i, j);
         R dby;
@@ -423,10 +424,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         val = in[5][idx] + dt * dby;
         if (STAGE == 2) val = R(0.75) * u0[5][idx] + R(0.25) * val;
         if (STAGE == 3) val = R(1.0 / 3.0) * u0[5][idx] + R(2.0 / 3.0) * val;
-        sBy[(lj + 1) * G::BYW + li] = val;
+        if (STAGE == 3) sBy[(lj + 1) * G::BYW + li] = val;
+        else out[5][idx] = val;
       }
     }
-    __syncthreads();
+    if (STAGE == 3) __syncthreads();   // stages 1, 2 read no phase-3a result in phase 3b
 
     // ---- phase 3b: cell update -------------------------------------------------
     double e_speed = 0.0, e_dmax = 0.0, e_dsum = 0.0, e_bmax = 0.0, e_mass = 0.0, e_en = 0.0;
@@ -485,12 +487,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         for (int q = 0; q < 4; ++q) U[q] = R(1.0 / 3.0) * u0[q][idx] + R(2.0 / 3.0) * U[q];
       }
       if (STAGE >= 2) floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
-      const R bxn = sBx[lj * G::BXW + (li + 1)];
-      const R byn = sBy[(lj + 1) * G::BYW + li];
 #pragma unroll
       for (int q = 0; q < 4; ++q) out[q][idx] = U[q];
-      out[4][idx] = bxn;
-      out[5][idx] = byn;
+      const R bxn = (STAGE == 3) ? sBx[lj * G::BXW + (li + 1)] : R(0);
+      const R byn = (STAGE == 3) ? sBy[(lj + 1) * G::BYW + li] : R(0);
+      if (STAGE == 3) {   // (stages 1, 2 stored the new face B in phase 3a)
+        out[4][idx] = bxn;
+        out[5][idx] = byn;
+      }
 
       if (STAGE == 3) {
         // epilogue: primitives of U^{n+1} (next step's CFL, src/main.f90:69-79),
