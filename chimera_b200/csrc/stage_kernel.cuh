@@ -134,6 +134,44 @@ __device__ __forceinline__ double block_reduce_max(double v, double* red) {
   return r;
 }
 
+// The six per-tile partials (max CFL speed, max |div B|, sum |div B|, max
+// |B|, mass, energy) reduced over the block in one pass: each value takes the
+// same shuffle tree and the same warp order as block_reduce_max / _sum, with
+// one barrier instead of twelve.  red holds [6][NT / 32]; the results are
+// valid on thread 0.
+template <int NT>
+__device__ __forceinline__ void block_reduce_partials(double (&v)[6], double* red) {
+  constexpr int NW = NT / 32;
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] = fmax(v[0], __shfl_down_sync(0xffffffffu, v[0], o));
+    v[1] = fmax(v[1], __shfl_down_sync(0xffffffffu, v[1], o));
+    v[2] += __shfl_down_sync(0xffffffffu, v[2], o);
+    v[3] = fmax(v[3], __shfl_down_sync(0xffffffffu, v[3], o));
+    v[4] += __shfl_down_sync(0xffffffffu, v[4], o);
+    v[5] += __shfl_down_sync(0xffffffffu, v[5], o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k * NW + w] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    v[0] = red[0 * NW]; v[1] = red[1 * NW]; v[3] = red[3 * NW];
+    v[2] = 0.0; v[4] = 0.0; v[5] = 0.0;
+    for (int k = 0; k < NW; ++k) {
+      if (k > 0) {
+        v[0] = fmax(v[0], red[0 * NW + k]);
+        v[1] = fmax(v[1], red[1 * NW + k]);
+        v[3] = fmax(v[3], red[3 * NW + k]);
+      }
+      v[2] += red[2 * NW + k];
+      v[4] += red[4 * NW + k];
+      v[5] += red[5 * NW + k];
+    }
+  }
+}
+
 // Per-cell CFL speed cf + |v| (src/main.f90:72-79), FP64.
 __device__ __forceinline__ double cfl_speed(double rho, double vx, double vy, double P, double Bx,
                                             double By, double gamma) {
@@ -230,7 +268,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   R* sFy = sFx + 5 * G::NFX;
   R* sBx = sFy + 5 * G::NFY;
   R* sBy = sBx + G::NBX;
-  __shared__ double red[NT / 32];
+  __shared__ double red[6 * (NT / 32)];
   __shared__ int s_last;
 
   const int tid = threadIdx.x;
@@ -522,15 +560,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     }
 
     if (STAGE == 3 && !a.dry) {
-      const double r0 = block_reduce_max<NT>(e_speed, red);
-      const double r1 = block_reduce_max<NT>(e_dmax, red);
-      const double r2 = block_reduce_sum<NT>(e_dsum, red);
-      const double r3 = block_reduce_max<NT>(e_bmax, red);
-      const double r4 = block_reduce_sum<NT>(e_mass, red);
-      const double r5 = block_reduce_sum<NT>(e_en, red);
+      double r[6] = {e_speed, e_dmax, e_dsum, e_bmax, e_mass, e_en};
+      block_reduce_partials<NT>(r, red);
       if (tid == 0) {
         double* p = a.partials + size_t(w) * NPART;
-        p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = r5;
+        p[0] = r[0]; p[1] = r[1]; p[2] = r[2]; p[3] = r[3]; p[4] = r[4]; p[5] = r[5];
         __threadfence();
         const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
         s_last = (prev == unsigned(g.tiles_x * g.tiles_y - 1)) ? 1 : 0;

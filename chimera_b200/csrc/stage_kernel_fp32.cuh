@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   R* sFy = sFx + 5 * G::NFX;                    // [5][NFY]
   R* sBx = sS;                                  // new face B (phase 3a on): reuses the slopes
   R* sBy = sBx + G::NBX;
-  __shared__ double red[NT / 32];
+  __shared__ double red[6 * (NT / 32)];
   __shared__ int s_last;
   __shared__ __align__(8) uint64_t s_bar;    // TMA completion
   // TMA pipeline state, kept in shared memory rather than in a register that
@@ -508,15 +508,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
     }
 
     if (STAGE == 3 && !a.dry) {
-      const double r0 = block_reduce_max<NT>(e_speed, red);
-      const double r1 = block_reduce_max<NT>(e_dmax, red);
-      const double r2 = block_reduce_sum<NT>(e_dsum, red);
-      const double r3 = block_reduce_max<NT>(e_bmax, red);
-      const double r4 = block_reduce_sum<NT>(e_mass, red);
-      const double r5 = block_reduce_sum<NT>(e_en, red);
+      double r[6] = {e_speed, e_dmax, e_dsum, e_bmax, e_mass, e_en};
+      block_reduce_partials<NT>(r, red);
       if (tid == 0) {
         double* p = a.partials + size_t(w) * NPART;
-        p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = r5;
+        p[0] = r[0]; p[1] = r[1]; p[2] = r[2]; p[3] = r[3]; p[4] = r[4]; p[5] = r[5];
         __threadfence();
         const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
         s_last = (prev == unsigned(g.tiles_x * g.tiles_y - 1)) ? 1 : 0;
