@@ -104,41 +104,11 @@ __device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_nex
   }
 }
 
-// Block-wide reductions (deterministic for a fixed block size).
-template <int NT>
-__device__ __forceinline__ double block_reduce_sum(double v, double* red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < NT / 32; ++k) r += red[k];
-  }
-  return r;  // valid on thread 0
-}
-
-template <int NT>
-__device__ __forceinline__ double block_reduce_max(double v, double* red) {
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (threadIdx.x == 0) {
-    r = red[0];
-    for (int k = 1; k < NT / 32; ++k) r = fmax(r, red[k]);
-  }
-  return r;
-}
-
 // The six per-tile partials (max CFL speed, max |div B|, sum |div B|, max
-// |B|, mass, energy) reduced over the block in one pass: each value takes the
-// same shuffle tree and the same warp order as block_reduce_max / _sum, with
-// one barrier instead of twelve.  red holds [6][NT / 32]; the results are
-// valid on thread 0.
+// |B|, mass, energy) reduced over the block in one pass, deterministically for
+// a fixed block size: a shuffle tree within each warp, then the warps in
+// order, with one barrier.  red holds [6][NT / 32]; the results are valid on
+// thread 0.
 template <int NT>
 __device__ __forceinline__ void block_reduce_partials(double (&v)[6], double* red) {
   constexpr int NW = NT / 32;
@@ -214,12 +184,9 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
     ms += __ldcg(p + 4);
     es += __ldcg(p + 5);
   }
-  sp = block_reduce_max<NT>(sp, red);
-  dmx = block_reduce_max<NT>(dmx, red);
-  dsum = block_reduce_sum<NT>(dsum, red);
-  bmx = block_reduce_max<NT>(bmx, red);
-  ms = block_reduce_sum<NT>(ms, red);
-  es = block_reduce_sum<NT>(es, red);
+  double r[6] = {sp, dmx, dsum, bmx, ms, es};
+  block_reduce_partials<NT>(r, red);
+  sp = r[0]; dmx = r[1]; dsum = r[2]; bmx = r[3]; ms = r[4]; es = r[5];
   if (threadIdx.x == 0) {
     double t = ctl->t;
     int oc = ctl->output_count;
@@ -585,7 +552,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
 // ----------------------------------------------------------------------------
 template <typename R, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
-  __shared__ double red[NT / 32];
+  __shared__ double red[6 * (NT / 32)];
   __shared__ int s_last;
   for (int w = a.work_begin + blockIdx.x; w < a.total_tiles; w += gridDim.x) {
     const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
@@ -618,15 +585,11 @@ __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
       ms += double(in[0][k]);
       es += double(in[3][k]);
     }
-    const double r0 = block_reduce_max<NT>(sp, red);
-    const double r1 = block_reduce_max<NT>(dmx, red);
-    const double r2 = block_reduce_sum<NT>(dsum, red);
-    const double r3 = block_reduce_max<NT>(bmx, red);
-    const double r4 = block_reduce_sum<NT>(ms, red);
-    const double r5 = block_reduce_sum<NT>(es, red);
+    double r[6] = {sp, dmx, dsum, bmx, ms, es};
+    block_reduce_partials<NT>(r, red);
     if (threadIdx.x == 0) {
       double* p = a.partials + size_t(w) * NPART;
-      p[0] = r0; p[1] = r1; p[2] = r2; p[3] = r3; p[4] = r4; p[5] = r5;
+      p[0] = r[0]; p[1] = r[1]; p[2] = r[2]; p[3] = r[3]; p[4] = r[4]; p[5] = r[5];
       __threadfence();
       const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
       s_last = (prev == unsigned(g.tiles_x * g.tiles_y - 1)) ? 1 : 0;
