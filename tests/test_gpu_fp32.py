@@ -160,3 +160,23 @@ def test_fp32_tma_variants_match_plain_loads(G, case):
             for q in range(6):
                 assert np.array_equal(a[q], b[q]), (case, plain, tma, q)
     s.close()
+
+
+def test_fp32_tma_variant_graph_replay_equals_eager(G):
+    """A TMA variant replayed from a captured CUDA graph gives the eager bits."""
+    cfg, st = P.orszag_tang(256)
+    c32 = cfg.replace(precision=FP32_BULK)
+    outs = []
+    for graph in (0, 5):
+        s = G.Solver(c32)
+        s.set_state(st)
+        s.set_variant(9)                       # 32 x 16 tiles, TMA box loads
+        if graph:
+            s.set_graph_steps(graph)
+        for _ in range(4):
+            s.step(5)
+        outs.append(s.get_state())
+        assert s.diag()["status"] == 0
+        s.close()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
