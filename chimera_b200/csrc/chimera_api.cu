@@ -230,6 +230,52 @@ static int ensure_dt(chimera_handle* h) {
   return CHIMERA_OK;
 }
 
+// Ghost rows of a y-slab (one grid split across ranks): copy `rows` whole rows
+// of every field of the current state (the buffer the device-side parity names)
+// to or from packed [field 6][rows][nx] buffers.  Pack: lo <- rows [rows, 2 rows),
+// hi <- rows [ny - 2 rows, ny - rows) (the interior rows a neighbour needs);
+// unpack: rows [0, rows) <- lo, rows [ny - rows, ny) <- hi.  A null side is skipped.
+template <typename T>
+__global__ void halo_rows_kernel(const Member* members, const Control* ctl, int rows, T* lo, T* hi,
+                                 int unpack) {
+  const Member& g = members[0];
+  const int side = blockIdx.z;
+  T* pk = side ? hi : lo;
+  if (!pk) return;
+  const int q = blockIdx.y;
+  const int nx = g.nx, ny = g.ny;
+  const int r0 = unpack ? (side ? ny - rows : 0) : (side ? ny - 2 * rows : rows);
+  T* st = reinterpret_cast<T*>(g.buf[ctl->parity][q]) + size_t(r0) * nx;
+  const size_t n = size_t(rows) * nx;
+  pk += size_t(q) * n;
+  for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+    if (unpack) st[k] = pk[k];
+    else pk[k] = st[k];
+  }
+}
+
+static int halo_rows(chimera_handle* h, int rows, void* lo, void* hi, int unpack) {
+  if (!h || rows < 1 || (!lo && !hi)) return CHIMERA_ERR_BAD_ARG;
+  if (h->n != 1) return CHIMERA_ERR_UNSUPPORTED;
+  const chimera_cfg& c = h->cfg[0];
+  if (2 * rows > c.ny) return CHIMERA_ERR_BAD_ARG;
+  const int eb = h->ks.elem_bytes;
+  if ((uintptr_t(lo) % eb) || (uintptr_t(hi) % eb)) return CHIMERA_ERR_BAD_ARG;
+  const size_t n = size_t(rows) * c.nx;
+  const dim3 grid(unsigned(std::min<size_t>((n + 255) / 256, 1024)), 6, 2);
+  if (eb == 8)
+    halo_rows_kernel<unsigned long long><<<grid, 256, 0, h->stream>>>(
+        h->d_members, h->d_ctl, rows, static_cast<unsigned long long*>(lo), static_cast<unsigned long long*>(hi),
+        unpack);
+  else
+    halo_rows_kernel<unsigned><<<grid, 256, 0, h->stream>>>(h->d_members, h->d_ctl, rows,
+                                                             static_cast<unsigned*>(lo),
+                                                             static_cast<unsigned*>(hi), unpack);
+  CK(cudaGetLastError());
+  if (unpack) h->dt_valid[0] = false;
+  return CHIMERA_OK;
+}
+
 static int one_step(chimera_handle* h) {
   for (int s = 0; s < 3; ++s) {
     int rc = launch(h, h->ks.stage[h->riemann - 1][s], h->grid_stage[s], s + 1);
@@ -894,6 +940,45 @@ int chimera_set_counters(chimera_handle* h, int on) {
   if (!h) return CHIMERA_ERR_BAD_ARG;
   h->counters = on ? 1 : 0;
   drop_graph(h);
+  return CHIMERA_OK;
+}
+
+int chimera_halo_pack(chimera_handle* h, int rows, void* lo, void* hi) {
+  return halo_rows(h, rows, lo, hi, 0);
+}
+
+int chimera_halo_unpack(chimera_handle* h, int rows, const void* lo, const void* hi) {
+  return halo_rows(h, rows, const_cast<void*>(lo), const_cast<void*>(hi), 1);
+}
+
+int chimera_slab_ghost_rows(chimera_handle* h, int ghost_lo, int ghost_hi) {
+  if (!h || ghost_lo < 0 || ghost_hi < 0) return CHIMERA_ERR_BAD_ARG;
+  if (h->n != 1) return CHIMERA_ERR_UNSUPPORTED;
+  if (ghost_lo + ghost_hi >= h->cfg[0].ny) return CHIMERA_ERR_BAD_ARG;
+  h->hm[0].skip_lo = ghost_lo;
+  h->hm[0].skip_hi = ghost_hi;
+  CK(cudaMemcpyAsync(h->d_members, h->hm.data(), sizeof(Member) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->dt_valid[0] = false;
+  return CHIMERA_OK;
+}
+
+int chimera_refresh_dt(chimera_handle* h, double* d_dt) {
+  if (!h) return CHIMERA_ERR_BAD_ARG;
+  for (int m = 0; m < h->n; ++m) h->dt_valid[m] = false;
+  int rc = ensure_dt(h);
+  if (rc) return rc;
+  if (d_dt)   // member m's Control::dt -> d_dt[m]
+    CK(cudaMemcpy2DAsync(d_dt, sizeof(double), &h->d_ctl[0].dt, sizeof(Control), sizeof(double), h->n,
+                         cudaMemcpyDeviceToDevice, h->stream));
+  return CHIMERA_OK;
+}
+
+int chimera_set_dt_device(chimera_handle* h, const double* d_dt) {
+  if (!h || !d_dt) return CHIMERA_ERR_BAD_ARG;
+  CK(cudaMemcpy2DAsync(&h->d_ctl[0].dt, sizeof(Control), d_dt, sizeof(double), sizeof(double), h->n,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  for (int m = 0; m < h->n; ++m) h->dt_valid[m] = true;
   return CHIMERA_OK;
 }
 

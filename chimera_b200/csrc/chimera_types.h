@@ -30,6 +30,8 @@ struct Member {
   double gamma, vol, len;  // vol = dx*dy, len = min(dx, dy)
   double inv_vol;          // 1/vol (FP32-bulk pressure recovery)
   double courant, t_out, t_end;
+  int skip_lo, skip_hi;     // rows at the bottom / top that the CFL kernel's dt and diagnostics
+                           // leave out (the ghost rows of a y-slab; 0 otherwise)
   void* buf[3][6];
   const void* tmap;        // TMA variants: this member's tensor maps [buffer 3][field 6] (CUtensorMap,
                            // 128 bytes each, boxes of the variant's tile) in device memory, or null

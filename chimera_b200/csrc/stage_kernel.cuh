@@ -154,6 +154,21 @@ __device__ __forceinline__ double cfl_speed(double rho, double vx, double vy, do
 }
 
 // divB of one cell from face values (src/mhd_field_ops.f90:60-117).
+// FP32-bulk form: a cell's CFL speed c_f + |v| (FP64 pressure recovery, FP32
+// wave speeds) and |B|.  The stage-3 epilogue and the CFL kernel both use it,
+// so that a dt is the same whichever of the two computed it.
+__device__ __forceinline__ void speed_f32(float M, float Mx, float My, float E, float Bx, float By,
+                                          const Member& g, double& speed, double& bmag) {
+  const Prim<float> pr = get_primitive_mixed(M, Mx, My, E, Bx, By, g.gamma, g.inv_vol, float(g.inv_vol));
+  const float gamma = float(g.gamma);
+  const float inv_rho = 1.0f / pr.rho;
+  const float B2 = Bx * Bx + By * By;
+  float cf = sqrtf(gamma * (pr.P - 0.5f * B2) * inv_rho + B2 * inv_rho);
+  if (pr.rho < 1.0e-3f) cf = fminf(cf, 50.0f);
+  speed = double(cf + sqrtf(pr.vx * pr.vx + pr.vy * pr.vy));
+  bmag = double(sqrtf(B2));
+}
+
 __device__ __forceinline__ double divb_cell(double bx, double bxm, double by, double bym, bool has_x,
                                             bool has_y, double inv_dx, double inv_dy, bool square) {
   if (square) {
@@ -567,21 +582,31 @@ __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
     double sp = 0.0, dmx = 0.0, dsum = 0.0, bmx = 0.0, ms = 0.0, es = 0.0;
     for (int c = threadIdx.x; c < TX * TY; c += NT) {
       const int i = i0 + c % TX, j = j0 + c / TX;
-      if (i >= nx || j >= ny) continue;
+      if (i >= nx || j >= ny - g.skip_hi || j < g.skip_lo) continue;
       const size_t k = size_t(j) * nx + i;
-      const double bxc = double(in[4][k]), byc = double(in[5][k]);
       const bool hx = (i > 0) || g.periodic_x, hy = (j > 0) || g.periodic_y;
-      const double bxm = hx ? double(in[4][(i > 0) ? k - 1 : k + (nx - 1)]) : bxc;
-      const double bym = hy ? double(in[5][(j > 0) ? k - nx : k + size_t(ny - 1) * nx]) : byc;
-      const double Bx = hx ? 0.5 * (bxc + bxm) : bxc;
-      const double By = hy ? 0.5 * (byc + bym) : byc;
-      Prim<double> pr = get_primitive<double>(double(in[0][k]), double(in[1][k]), double(in[2][k]),
-                                              double(in[3][k]), Bx, By, g.gamma, g.vol);
-      sp = fmax(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+      const R bxr = in[4][k], byr = in[5][k];
+      const R bxmr = hx ? in[4][(i > 0) ? k - 1 : k + (nx - 1)] : bxr;
+      const R bymr = hy ? in[5][(j > 0) ? k - nx : k + size_t(ny - 1) * nx] : byr;
+      const double bxc = double(bxr), byc = double(byr), bxm = double(bxmr), bym = double(bymr);
+      if constexpr (sizeof(R) == 4) {   // the FP32-bulk epilogue's arithmetic
+        const R Bx = hx ? R(0.5) * (bxr + bxmr) : bxr;
+        const R By = hy ? R(0.5) * (byr + bymr) : byr;
+        double spc, bm;
+        speed_f32(in[0][k], in[1][k], in[2][k], in[3][k], Bx, By, g, spc, bm);
+        sp = fmax(sp, spc);
+        bmx = fmax(bmx, bm);
+      } else {
+        const double Bx = hx ? 0.5 * (bxc + bxm) : bxc;
+        const double By = hy ? 0.5 * (byc + bym) : byc;
+        Prim<double> pr = get_primitive<double>(double(in[0][k]), double(in[1][k]), double(in[2][k]),
+                                                double(in[3][k]), Bx, By, g.gamma, g.vol);
+        sp = fmax(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+        bmx = fmax(bmx, sqrt(Bx * Bx + By * By));
+      }
       const double d = fabs(divb_cell(bxc, bxm, byc, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
       dmx = fmax(dmx, d);
       dsum += d;
-      bmx = fmax(bmx, sqrt(Bx * Bx + By * By));
       ms += double(in[0][k]);
       es += double(in[3][k]);
     }

@@ -486,18 +486,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const bool hx = (i > 0) || px, hy = (j > 0) || py;
         const R Bx = hx ? R(0.5) * (bxn + bxm) : bxn;
         const R By = hy ? R(0.5) * (byn + bym) : byn;
-        const Prim<R> pr = get_primitive_mixed(U[0], U[1], U[2], U[3], Bx, By, g.gamma, g.inv_vol,
-                                               float(g.inv_vol));
-        const R inv_rho = R(1) / pr.rho;
-        const R B2 = Bx * Bx + By * By;
-        R cf = sqrtf(gamma * (pr.P - R(0.5) * B2) * inv_rho + B2 * inv_rho);
-        if (pr.rho < R(1.0e-3)) cf = fminf(cf, R(50));
-        e_speed = fmax(e_speed, double(cf + sqrtf(pr.vx * pr.vx + pr.vy * pr.vy)));
+        double spc, bm;
+        speed_f32(U[0], U[1], U[2], U[3], Bx, By, g, spc, bm);
+        e_speed = fmax(e_speed, spc);
         const double dv = fabs(divb_cell(double(bxn), double(bxm), double(byn), double(bym), hx, hy,
                                          g.inv_dx, g.inv_dy, g.square != 0));
         e_dmax = fmax(e_dmax, dv);
         e_dsum += dv;
-        e_bmax = fmax(e_bmax, double(sqrtf(B2)));
+        e_bmax = fmax(e_bmax, bm);
         e_mass += double(U[0]);
         e_en += double(U[3]);
       }

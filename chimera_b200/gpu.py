@@ -97,6 +97,11 @@ def lib():
                                           C.POINTER(C.c_int)]
         L.chimera_stream.argtypes = [P]
         L.chimera_stream.restype = P
+        L.chimera_halo_pack.argtypes = [P, C.c_int, P, P]
+        L.chimera_halo_unpack.argtypes = [P, C.c_int, P, P]
+        L.chimera_slab_ghost_rows.argtypes = [P, C.c_int, C.c_int]
+        L.chimera_refresh_dt.argtypes = [P, P]
+        L.chimera_set_dt_device.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -265,6 +270,31 @@ class Solver:
 
     def set_variant(self, v: int):
         _check(lib().chimera_set_variant(self._h, int(v)), "set_variant")
+
+    # ---- y-slab decomposition (chimera_halo_pack / _unpack, chimera_refresh_dt,
+    # chimera_set_dt_device): asynchronous on the handle's stream, device tensors only
+    @staticmethod
+    def _dev_ptr(t):
+        if t is None:
+            return None
+        if not (hasattr(t, "is_cuda") and t.is_cuda and t.is_contiguous()):
+            raise ValueError("expected a contiguous CUDA tensor")
+        return C.c_void_p(t.data_ptr())
+
+    def halo_pack(self, rows: int, lo=None, hi=None):
+        _check(lib().chimera_halo_pack(self._h, int(rows), self._dev_ptr(lo), self._dev_ptr(hi)), "halo_pack")
+
+    def halo_unpack(self, rows: int, lo=None, hi=None):
+        _check(lib().chimera_halo_unpack(self._h, int(rows), self._dev_ptr(lo), self._dev_ptr(hi)), "halo_unpack")
+
+    def slab_ghost_rows(self, ghost_lo: int, ghost_hi: int):
+        _check(lib().chimera_slab_ghost_rows(self._h, int(ghost_lo), int(ghost_hi)), "slab_ghost_rows")
+
+    def refresh_dt(self, dt=None):
+        _check(lib().chimera_refresh_dt(self._h, self._dev_ptr(dt)), "refresh_dt")
+
+    def set_dt_device(self, dt):
+        _check(lib().chimera_set_dt_device(self._h, self._dev_ptr(dt)), "set_dt_device")
 
     def variant(self):
         v, tx, ty, nt = C.c_int(), C.c_int(), C.c_int(), C.c_int()

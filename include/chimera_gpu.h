@@ -190,6 +190,38 @@ int chimera_variant_count(chimera_handle* h);
 int chimera_set_variant(chimera_handle* h, int variant);
 int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_y, int* threads);
 
+/* ---- one grid split into y-slabs across ranks (no counterpart in the reference) --
+ * The reference advances one grid in one process (src/main.f90:65-303).  A
+ * slab handle holds its rows of the grid plus `rows` ghost rows on each side
+ * that has a neighbour.  Once per step the caller (i) packs the interior rows
+ * its neighbours need, (ii) moves them (NCCL send / recv, or a copy when the
+ * slabs share a GPU), (iii) unpacks the received ghost rows, (iv) computes the
+ * slab's CFL dt into a device double, (v) takes the minimum over the slabs
+ * (an all-reduce) and (vi) writes it back before chimera_step(h, 1).  Seven
+ * ghost rows make every interior cell of the step identical to the undivided
+ * grid's: each RK3 stage reaches two rows, and the lowest ghost row is wrong
+ * before the first stage (its cell-centred B averages a face below it that
+ * the slab does not hold), so 1 + 3 x 2 rows at the bottom (6 at the top).
+ * Single-member handles only; the per-step calls are asynchronous on the
+ * handle's stream.
+ *   - pack:   lo <- state rows [rows, 2 rows), hi <- rows [ny - 2 rows, ny - rows)
+ *   - unpack: state rows [0, rows) <- lo, rows [ny - rows, ny) <- hi
+ * lo / hi are device buffers of 6 * rows * nx elements (field-major, Mass..b_y),
+ * 8-byte elements for CHIMERA_FP64 and 4-byte ones for CHIMERA_FP32_BULK; a
+ * null side is skipped.  Requires 2 * rows <= ny. */
+int chimera_halo_pack(chimera_handle* h, int rows, void* lo, void* hi);
+int chimera_halo_unpack(chimera_handle* h, int rows, const void* lo, const void* hi);
+/* Declare the ghost rows (bottom, top) of a slab handle: the CFL dt and the
+ * diagnostics of chimera_refresh_dt (and chimera_diag right after it) cover
+ * only the slab's own rows, so that the minimum / maximum / sum over the
+ * slabs is the grid's.  Synchronises. */
+int chimera_slab_ghost_rows(chimera_handle* h, int ghost_lo, int ghost_hi);
+/* CFL dt of the current state (src/main.f90:69-83, with the tOut clip) into
+ * d_dt[member] (device memory; null: only the handle's own copy). */
+int chimera_refresh_dt(chimera_handle* h, double* d_dt);
+/* Set every member's dt from d_dt[member] (device memory) for the next step. */
+int chimera_set_dt_device(chimera_handle* h, const double* d_dt);
+
 /* ---- discrete adjoint of one RK3 step (FP64, periodic) -------------------------
  * No counterpart in the reference.  lambda_n = (dU_{n+1}/dU_n)^T lambda_{n+1}
  * for the step U_n -> U_{n+1} with a given (frozen) dt: the MOOD, floor and
