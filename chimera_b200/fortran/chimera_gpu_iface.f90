@@ -15,6 +15,13 @@ module chimera_gpu_iface
     public :: chimera_batch_create, chimera_batch_set_state, chimera_batch_get_state
     public :: chimera_batch_set_time, chimera_batch_diag, chimera_set_graph_steps
     public :: chimera_autotune, chimera_set_variant
+    public :: chimera_halo_pack, chimera_halo_unpack, chimera_slab_ghost_rows
+    public :: chimera_refresh_dt, chimera_set_dt_device
+    public :: chimera_stage, chimera_get_stage_buffer, chimera_set_counters, chimera_set_profiling
+    public :: chimera_get_profile, chimera_stream, chimera_batch_size, chimera_variant_count
+    public :: chimera_get_variant, chimera_rk3_step_noalloc, chimera_strerror, chimera_version
+    public :: chimera_adjoint_create, chimera_adjoint_step, chimera_adjoint_forward_step
+    public :: chimera_adjoint_destroy
     public :: chimera_op_average_face_to_cell_B, chimera_op_get_primitive, chimera_op_get_conserved
     public :: chimera_op_apply_conserved_floors, chimera_op_fill_ghost_cells
     public :: chimera_op_compute_gradients, chimera_op_apply_slope_limiter, chimera_op_reconstruction
@@ -168,6 +175,147 @@ module chimera_gpu_iface
             import :: c_int, c_ptr
             type(c_ptr), value :: h
             integer(c_int), value :: variant
+        end function
+
+        ! ---- one grid split into y-slabs across ranks (an MPI or NCCL caller moves
+        !      the packed ghost rows and takes the minimum dt between the calls) --------
+        integer(c_int) function chimera_halo_pack(h, rows, lo, hi) bind(C, name="chimera_halo_pack")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, lo, hi
+            integer(c_int), value :: rows
+        end function
+
+        integer(c_int) function chimera_halo_unpack(h, rows, lo, hi) bind(C, name="chimera_halo_unpack")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, lo, hi
+            integer(c_int), value :: rows
+        end function
+
+        integer(c_int) function chimera_slab_ghost_rows(h, ghost_lo, ghost_hi) &
+                bind(C, name="chimera_slab_ghost_rows")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int), value :: ghost_lo, ghost_hi
+        end function
+
+        ! ---- stage-level access, counters, timing, tile variants ------------------------
+        integer(c_int) function chimera_stage(h, k, dt) bind(C, name="chimera_stage")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            integer(c_int), value :: k
+            real(c_double), value :: dt
+        end function
+
+        integer(c_int) function chimera_get_stage_buffer(h, b, Mass, Momx, Momy, Energy, b_x, b_y, ld, where) &
+                bind(C, name="chimera_get_stage_buffer")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            integer(c_int), value :: b
+            real(c_double), intent(out) :: Mass(*), Momx(*), Momy(*), Energy(*), b_x(*), b_y(*)
+            integer(c_int), value :: ld, where
+        end function
+
+        integer(c_int) function chimera_set_counters(h, on) bind(C, name="chimera_set_counters")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int), value :: on
+        end function
+
+        integer(c_int) function chimera_set_profiling(h, on) bind(C, name="chimera_set_profiling")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int), value :: on
+        end function
+
+        integer(c_int) function chimera_get_profile(h, ms, launches, reset) bind(C, name="chimera_get_profile")
+            import :: c_int, c_ptr, c_double, c_long_long
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: ms(4)
+            integer(c_long_long), intent(out) :: launches(4)
+            integer(c_int), value :: reset
+        end function
+
+        type(c_ptr) function chimera_stream(h) bind(C, name="chimera_stream")
+            import :: c_ptr
+            type(c_ptr), value :: h
+        end function
+
+        integer(c_int) function chimera_batch_size(h) bind(C, name="chimera_batch_size")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+
+        integer(c_int) function chimera_variant_count(h) bind(C, name="chimera_variant_count")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+
+        integer(c_int) function chimera_get_variant(h, variant, tile_x, tile_y, threads) &
+                bind(C, name="chimera_get_variant")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int), intent(out) :: variant, tile_x, tile_y, threads
+        end function
+
+        ! ---- one step without device allocation (device arrays updated in place) --------
+        integer(c_int) function chimera_rk3_step_noalloc(cfg, Mass, Momx, Momy, Energy, b_x, b_y, t, &
+                output_count, dt_next, stream) bind(C, name="chimera_rk3_step_noalloc")
+            import :: c_int, c_ptr, c_double, chimera_cfg
+            type(chimera_cfg), intent(in) :: cfg
+            type(c_ptr), value :: Mass, Momx, Momy, Energy, b_x, b_y
+            real(c_double), intent(inout) :: t
+            integer(c_int), intent(inout) :: output_count
+            real(c_double), intent(out) :: dt_next
+            type(c_ptr), value :: stream
+        end function
+
+        ! ---- discrete adjoint of one RK3 step (arrays of six device pointers) ------------
+        integer(c_int) function chimera_adjoint_create(cfg, stream, a) bind(C, name="chimera_adjoint_create")
+            import :: c_int, c_ptr, chimera_cfg
+            type(chimera_cfg), intent(in) :: cfg
+            type(c_ptr), value :: stream
+            type(c_ptr), intent(out) :: a
+        end function
+
+        integer(c_int) function chimera_adjoint_step(a, U_n, dt, lambda_next, lambda_n) &
+                bind(C, name="chimera_adjoint_step")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: a
+            type(c_ptr), intent(in) :: U_n(6), lambda_next(6), lambda_n(6)
+            real(c_double), value :: dt
+        end function
+
+        integer(c_int) function chimera_adjoint_forward_step(a, U_n, dt, U_next) &
+                bind(C, name="chimera_adjoint_forward_step")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: a
+            type(c_ptr), intent(in) :: U_n(6), U_next(6)
+            real(c_double), value :: dt
+        end function
+
+        subroutine chimera_adjoint_destroy(a) bind(C, name="chimera_adjoint_destroy")
+            import :: c_ptr
+            type(c_ptr), value :: a
+        end subroutine
+
+        ! ---- error text (a C string: c_f_pointer it to a character array) and version ----
+        type(c_ptr) function chimera_strerror(code) bind(C, name="chimera_strerror")
+            import :: c_int, c_ptr
+            integer(c_int), value :: code
+        end function
+
+        integer(c_int) function chimera_version() bind(C, name="chimera_version")
+            import :: c_int
+        end function
+
+        integer(c_int) function chimera_refresh_dt(h, d_dt) bind(C, name="chimera_refresh_dt")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, d_dt
+        end function
+
+        integer(c_int) function chimera_set_dt_device(h, d_dt) bind(C, name="chimera_set_dt_device")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, d_dt
         end function
 
         ! ---- per-routine entry points: device arrays (c_ptr from the caller's allocator),

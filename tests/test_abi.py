@@ -72,3 +72,34 @@ def test_null_arguments(lib):
     assert lib.chimera_step(None, 1) == -1
     assert lib.chimera_diag(None, None) == -1
     lib.chimera_destroy(None)
+
+
+FORTRAN = os.path.join(ROOT, "chimera_b200", "fortran", "chimera_gpu_iface.f90")
+
+
+def _c_arities(path):
+    """name -> number of parameters of every prototype in the header."""
+    text = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(chimera_\w+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        p = params.strip()
+        out[name] = 0 if p in ("", "void") else p.count(",") + 1
+    return out
+
+
+def _fortran_arities(path):
+    """bind(C) name -> number of dummy arguments in the interface module."""
+    text = open(path).read().replace("&\n", " ")
+    out = {}
+    for args, name in re.findall(r"(?:function|subroutine)\s+\w+\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)",
+                                 text):
+        out[name] = len([a for a in args.split(",") if a.strip()])
+    return out
+
+
+def test_fortran_module_binds_every_entry_point_with_its_arity():
+    c, f = _c_arities(HEADER), _fortran_arities(FORTRAN)
+    assert set(c) == set(declared_symbols(HEADER))
+    assert sorted(set(c) - set(f)) == []
+    assert sorted(set(f) - set(c)) == []
+    assert {k: f[k] for k in c if f[k] != c[k]} == {}
