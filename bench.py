@@ -61,6 +61,9 @@ def parse():
     p.add_argument("--kh-steps", type=int, default=1000)
     p.add_argument("--adjoint", choices=("on", "off"), default="on",
                    help="also measure the field-loop adjoint (forward + backward, central differences)")
+    p.add_argument("--slabs", type=int, default=0,
+                   help="also run the FP64 Kelvin-Helmholtz grid as this many y-slabs on one GPU "
+                        "(ghost-row exchange by device copies) against the undivided grid (0: off)")
     p.add_argument("--variant", type=int, default=-1,
                    help="force a tile variant for the single-grid measurement (-1: autotune)")
     return p.parse_args()
@@ -382,6 +385,7 @@ def run_chimera(args, world, rank, local):
         kh = run_kh(args)
     if world == 1 and args.adjoint == "on":
         adj_leg = run_adjoint_leg(args)
+    slab_leg = run_slab_leg(args) if world == 1 and args.slabs > 1 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -421,6 +425,7 @@ def run_chimera(args, world, rank, local):
             "forms": ens,
             "kelvin_helmholtz": kh,
             "adjoint": adj_leg,
+            "slabs": slab_leg,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -578,6 +583,53 @@ def run_kh(args):
     res["workload"] = (f"Kelvin-Helmholtz {n}^2 on [0,1]x[-1,1], periodic, HLLD + MC + MOOD, gamma 1.4, "
                        f"{steps} RK3 steps from the same state")
     return res
+
+
+def run_slab_leg(args):
+    """The FP64 Kelvin-Helmholtz grid (HLLD + MC + MOOD) as ``args.slabs``
+    y-slabs on one GPU -- separate handles on one stream, 7 ghost rows moved
+    by device copies and the dt minimum taken every step (chimera_b200.slab)
+    -- against the undivided grid stepped eagerly from the same state: device
+    time per step of each, the overhead of the decomposition (redundant ghost
+    rows, pack / unpack, the dt hand-off, smaller launches) and whether the
+    results are bitwise equal."""
+    import numpy as np
+    import torch
+    from chimera_b200 import gpu, problems
+    from chimera_b200.slab import LocalTransport, SlabSolver, gather_interior, slab_step
+    n, k, steps = args.kh_n, args.slabs, 50
+    cfg, st = problems.kelvin_helmholtz(n)
+    whole = gpu.Solver(cfg)
+    whole.set_state(st)
+    whole.step(3)                                         # warm-up (not timed)
+    whole.set_state(st)
+    whole.set_time(0.0, 1)
+    whole.step(0)
+    ms_whole = _timed_run(whole, steps, 1)
+    ref = whole.get_state()
+    whole.close()
+    stream = torch.cuda.Stream()
+    slabs = [SlabSolver(cfg, r, k, stream=stream) for r in range(k)]
+    for sl in slabs:
+        sl.set_global_state(st)
+    slab_step(slabs, LocalTransport(), 3)                  # warm-up (not timed)
+    for sl in slabs:
+        sl.set_global_state(st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    slab_step(slabs, LocalTransport(), steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms_slabs = e0.elapsed_time(e1)
+    got = gather_interior(slabs)
+    for sl in slabs:
+        sl.close()
+    return {"workload": f"Kelvin-Helmholtz {n}^2 FP64, HLLD + MC + MOOD, {steps} RK3 steps, "
+                        f"{k} y-slabs of about {n // k} rows + 7 ghost rows per neighbour, on one GPU",
+            "slabs": k, "ms_per_step_slabs": ms_slabs / steps, "ms_per_step_whole": ms_whole / steps,
+            "overhead": ms_slabs / ms_whole - 1.0,
+            "bitwise_equal": all(bool(np.array_equal(got[q], ref[q])) for q in range(6))}
 
 
 def run_adjoint_leg(args):

@@ -272,7 +272,9 @@ static int halo_rows(chimera_handle* h, int rows, void* lo, void* hi, int unpack
                                                              static_cast<unsigned*>(lo),
                                                              static_cast<unsigned*>(hi), unpack);
   CK(cudaGetLastError());
-  if (unpack) h->dt_valid[0] = false;
+  // the dt stays valid when only rows that its reduction leaves out changed
+  const Member& g = h->hm[0];
+  if (unpack && ((lo && rows > g.skip_lo) || (hi && rows > g.skip_hi))) h->dt_valid[0] = false;
   return CHIMERA_OK;
 }
 
@@ -971,6 +973,15 @@ int chimera_refresh_dt(chimera_handle* h, double* d_dt) {
   if (d_dt)   // member m's Control::dt -> d_dt[m]
     CK(cudaMemcpy2DAsync(d_dt, sizeof(double), &h->d_ctl[0].dt, sizeof(Control), sizeof(double), h->n,
                          cudaMemcpyDeviceToDevice, h->stream));
+  return CHIMERA_OK;
+}
+
+int chimera_get_dt_device(chimera_handle* h, double* d_dt) {
+  if (!h || !d_dt) return CHIMERA_ERR_BAD_ARG;
+  int rc = ensure_dt(h);
+  if (rc) return rc;
+  CK(cudaMemcpy2DAsync(d_dt, sizeof(double), &h->d_ctl[0].dt, sizeof(Control), sizeof(double), h->n,
+                       cudaMemcpyDeviceToDevice, h->stream));
   return CHIMERA_OK;
 }
 

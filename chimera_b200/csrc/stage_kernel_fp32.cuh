@@ -98,6 +98,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   R* sBy = sBx + G::NBX;
   __shared__ double red[6 * (NT / 32)];
   __shared__ int s_last;
+  __shared__ unsigned s_own;   // stage 3: bit r set if tile row r is one of the grid's own rows
+  static_assert(TY < 32, "the own-row mask holds one bit per tile row");
   __shared__ __align__(8) uint64_t s_bar;    // TMA completion
   // TMA pipeline state, kept in shared memory rather than in a register that
   // would stay live through the register-bound flux phase: bit 0 = this tile's
@@ -146,6 +148,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
     const int lt = w - g.tile_begin;
     const int i0 = (lt % g.tiles_x) * TX;
     const int j0 = (lt / g.tiles_x) * TY;
+    if (STAGE == 3 && tid == 0) {
+      // the tile rows whose cells enter the epilogue's reductions: all but a
+      // y-slab's ghost rows (read in phase 3b, after phase 1's barrier; the
+      // previous tile's reads ended before its closing barrier)
+      const int lo = min(max(g.skip_lo - j0, 0), TY), hi = min(max(ny - g.skip_hi - j0, 0), TY);
+      s_own = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+    }
     const R gamma = R(g.gamma);
     const R vol = R(g.vol);
     const R dt = R(ctl->dt);
@@ -480,7 +489,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         out[5][idx] = byn;
       }
 
-      if (STAGE == 3) {
+      if (STAGE == 3 && ((s_own >> lj) & 1u)) {   // a y-slab's ghost rows are left out
         const R bxm = sBx[lj * G::BXW + li];
         const R bym = sBy[lj * G::BYW + li];
         const bool hx = (i > 0) || px, hy = (j > 0) || py;

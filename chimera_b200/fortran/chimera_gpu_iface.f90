@@ -16,7 +16,7 @@ module chimera_gpu_iface
     public :: chimera_batch_set_time, chimera_batch_diag, chimera_set_graph_steps
     public :: chimera_autotune, chimera_set_variant
     public :: chimera_halo_pack, chimera_halo_unpack, chimera_slab_ghost_rows
-    public :: chimera_refresh_dt, chimera_set_dt_device
+    public :: chimera_refresh_dt, chimera_get_dt_device, chimera_set_dt_device
     public :: chimera_stage, chimera_get_stage_buffer, chimera_set_counters, chimera_set_profiling
     public :: chimera_get_profile, chimera_stream, chimera_batch_size, chimera_variant_count
     public :: chimera_get_variant, chimera_rk3_step_noalloc, chimera_strerror, chimera_version
@@ -309,6 +309,11 @@ module chimera_gpu_iface
         end function
 
         integer(c_int) function chimera_refresh_dt(h, d_dt) bind(C, name="chimera_refresh_dt")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, d_dt
+        end function
+
+        integer(c_int) function chimera_get_dt_device(h, d_dt) bind(C, name="chimera_get_dt_device")
             import :: c_int, c_ptr
             type(c_ptr), value :: h, d_dt
         end function

@@ -102,6 +102,7 @@ def lib():
         L.chimera_slab_ghost_rows.argtypes = [P, C.c_int, C.c_int]
         L.chimera_refresh_dt.argtypes = [P, P]
         L.chimera_set_dt_device.argtypes = [P, P]
+        L.chimera_get_dt_device.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -292,6 +293,9 @@ class Solver:
 
     def refresh_dt(self, dt=None):
         _check(lib().chimera_refresh_dt(self._h, self._dev_ptr(dt)), "refresh_dt")
+
+    def get_dt_device(self, dt):
+        _check(lib().chimera_get_dt_device(self._h, self._dev_ptr(dt)), "get_dt_device")
 
     def set_dt_device(self, dt):
         _check(lib().chimera_set_dt_device(self._h, self._dev_ptr(dt)), "set_dt_device")

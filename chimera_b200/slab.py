@@ -10,6 +10,9 @@ rank:
     ghost rows -> CFL dt of the slab's own rows -> minimum over the ranks ->
     the three RK3 stages (chimera_step)
 
+(the slab's dt for the next step comes from its stage-3 epilogue, which
+leaves the ghost rows out, so no separate CFL pass runs after the first step)
+
 Why GHOST = 7: the slab's ghost sides are declared outflow, and what that
 boundary does to the outer ghost rows spreads two rows per RK3 stage (slopes
 and MOOD bounds reach one row beyond a face's two cells).  At the bottom the
@@ -21,10 +24,11 @@ rows every interior cell, and the face b_y below the lowest interior cell,
 is bit-for-bit the undivided grid's.  (Six rows are not enough:
 tests/test_slab.py shows it.)
 
-The dt is exact: the CFL reduction of each slab covers only its own rows
-(chimera_slab_ghost_rows), the slabs' rows partition the grid, and the dt
-is a minimum (src/main.f90:72-83, the tOut clip is monotone), so the minimum
-over the slabs is the grid's dt.
+The dt is exact: the CFL reductions of each slab (its stage-3 epilogue and
+the CFL pass) cover only its own rows (chimera_slab_ghost_rows), whose
+values after a step are already the undivided grid's, the slabs' rows
+partition the grid, and the dt is a minimum (src/main.f90:72-83, the tOut
+clip is monotone), so the minimum over the slabs is the grid's dt.
 
 The exchange moves 2 x GHOST x nx x 6 values per slab and step (1.4 MB per
 side in FP64 at nx = 4096); nothing else crosses ranks.  Diagnostics
@@ -162,7 +166,9 @@ class SlabSolver:
             self.solver.halo_unpack(self.ghost, self.recv_lo, self.recv_hi)
 
     def refresh_dt(self):
-        self.solver.refresh_dt(self.dt)
+        # the dt the last stage 3 computed over the slab's own rows (a CFL pass
+        # before the first step); the ghost-row unpack does not change it
+        self.solver.get_dt_device(self.dt)
 
     def set_dt(self):
         self.solver.set_dt_device(self.dt)

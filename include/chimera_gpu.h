@@ -195,9 +195,11 @@ int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_
  * slab handle holds its rows of the grid plus `rows` ghost rows on each side
  * that has a neighbour.  Once per step the caller (i) packs the interior rows
  * its neighbours need, (ii) moves them (NCCL send / recv, or a copy when the
- * slabs share a GPU), (iii) unpacks the received ghost rows, (iv) computes the
- * slab's CFL dt into a device double, (v) takes the minimum over the slabs
- * (an all-reduce) and (vi) writes it back before chimera_step(h, 1).  Seven
+ * slabs share a GPU), (iii) unpacks the received ghost rows, (iv) fetches the
+ * slab's CFL dt into a device double (the previous step's stage 3 computed it
+ * over the slab's own rows, which the exchange leaves unchanged), (v) takes
+ * the minimum over the slabs (an all-reduce) and (vi) writes it back before
+ * chimera_step(h, 1).  Seven
  * ghost rows make every interior cell of the step identical to the undivided
  * grid's: each RK3 stage reaches two rows, and the lowest ghost row is wrong
  * before the first stage (its cell-centred B averages a face below it that
@@ -212,13 +214,19 @@ int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_
 int chimera_halo_pack(chimera_handle* h, int rows, void* lo, void* hi);
 int chimera_halo_unpack(chimera_handle* h, int rows, const void* lo, const void* hi);
 /* Declare the ghost rows (bottom, top) of a slab handle: the CFL dt and the
- * diagnostics of chimera_refresh_dt (and chimera_diag right after it) cover
+ * diagnostics (of the stage-3 epilogue, the CFL pass and chimera_diag) cover
  * only the slab's own rows, so that the minimum / maximum / sum over the
  * slabs is the grid's.  Synchronises. */
 int chimera_slab_ghost_rows(chimera_handle* h, int ghost_lo, int ghost_hi);
-/* CFL dt of the current state (src/main.f90:69-83, with the tOut clip) into
- * d_dt[member] (device memory; null: only the handle's own copy). */
+/* Recompute the CFL dt of the current state (src/main.f90:69-83, with the
+ * tOut clip; a CFL kernel launch) into d_dt[member] (device memory; null:
+ * only the handle's own copy), with the diagnostics of chimera_diag. */
 int chimera_refresh_dt(chimera_handle* h, double* d_dt);
+/* The dt the next step will use into d_dt[member] (device memory): the one
+ * the last stage 3 or CFL pass computed, or a CFL pass if the state changed
+ * since (a ghost-row unpack within chimera_slab_ghost_rows' rows does not
+ * count as a change). */
+int chimera_get_dt_device(chimera_handle* h, double* d_dt);
 /* Set every member's dt from d_dt[member] (device memory) for the next step. */
 int chimera_set_dt_device(chimera_handle* h, const double* d_dt);
 

@@ -121,3 +121,23 @@ def test_halo_rejects_bad_arguments(G):
     with pytest.raises(G.ChimeraError):
         b.halo_pack(2, buf, None)
     b.close()
+
+
+def test_slab_steps_take_dt_from_the_fused_epilogue(G):
+    """After the first step a slab's dt comes from its stage-3 epilogue (which
+    leaves the ghost rows out): one CFL kernel launch in all, and still the
+    undivided grid's result."""
+    cfg, st = P.orszag_tang(128)
+    ref, _ = _whole(G, cfg, st, 6)
+    stream = torch.cuda.Stream()
+    slabs = [SlabSolver(cfg, r, 3, stream=stream) for r in range(3)]
+    for s in slabs:
+        s.set_global_state(st)
+        s.solver.set_profiling(True)
+    slab_step(slabs, LocalTransport(), 6)
+    prof = [s.solver.get_profile() for s in slabs]
+    assert all(p["cfl"]["launches"] == 1 and p["stage3"]["launches"] == 6 for p in prof)
+    got = gather_interior(slabs)
+    assert all(np.array_equal(got[q], ref[q]) for q in range(6))
+    for s in slabs:
+        s.close()
