@@ -7,12 +7,12 @@
 namespace chimera {
 
 namespace {
-template <int TX, int TY, int NT, int MINB>
+template <int TX, int TY, int NT, int MINB, bool KEEP_IN = false>
 void fill(KernelSet* ks) {
   using G = TileGeom<TX, TY>;
-  const size_t smem = G::template smem_bytes<double>();
+  const size_t smem = G::template smem_bytes<double, KEEP_IN>();
 #define CHIMERA_ENTRY(S, K) \
-  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel<double, S, K, TX, TY, NT, MINB>, smem, TX, TY, NT}
+  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel<double, S, K, TX, TY, NT, MINB, KEEP_IN>, smem, TX, TY, NT}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
@@ -23,7 +23,7 @@ void fill(KernelSet* ks) {
 }  // namespace
 
 // Tile shapes and occupancy targets the autotuner chooses from.
-int fp64_variant_count() { return 5; }
+int fp64_variant_count() { return 6; }
 
 void fp64_kernels(int variant, KernelSet* out) {
   switch (variant) {
@@ -31,6 +31,7 @@ void fp64_kernels(int variant, KernelSet* out) {
     case 2: fill<32, 8, 128, 4>(out); break;
     case 3: fill<64, 8, 256, 2>(out); break;
     case 4: fill<16, 16, 128, 4>(out); break;
+    case 5: fill<32, 16, 256, 2, true>(out); break;   // phase 3b reads the stage input from shared memory
     default: fill<32, 16, 256, 1>(out); break;
   }
 }
