@@ -125,8 +125,13 @@ def to_ccfg(cfg: SolverConfig) -> CCfg:
                 int(bool(cfg.slope_limiting)), int(bool(cfg.mood)), int(getattr(cfg, "precision", 0)))
 
 
-def _ptrs(arrays, nx, ny):
-    """(pointers, ld, where, keepalive) for 6 arrays (numpy host or torch cuda)."""
+def _ptrs(arrays, nx, ny, out=False):
+    """(pointers, ld, where, keepalive) for 6 arrays (numpy host or torch cuda).
+
+    float64 arrays with unit x stride are passed as they are, with their row
+    pitch as ld (views of padded arrays included).  Other numpy inputs are
+    converted to a dense copy; an output (``out``) that would need a copy is
+    rejected, since the result would land in the copy."""
     ptrs, keep = [], []
     where = None
     ld = nx
@@ -140,11 +145,16 @@ def _ptrs(arrays, nx, ny):
             w = DEVICE if a.is_cuda else HOST
             ld_a, p = a.stride(0), a.data_ptr()
         else:
-            a = np.ascontiguousarray(a, dtype=np.float64)
-            if a.shape != (ny, nx):
-                raise ValueError(f"expected shape ({ny}, {nx}), got {a.shape}")
+            direct = (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.ndim == 2 and a.shape == (ny, nx)
+                      and a.strides[1] == 8 and a.strides[0] % 8 == 0 and a.strides[0] >= 8 * nx)
+            if not direct:
+                if out:
+                    raise ValueError(f"output arrays must be ({ny}, {nx}) float64 with unit x stride")
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                if a.shape != (ny, nx):
+                    raise ValueError(f"expected shape ({ny}, {nx}), got {a.shape}")
             keep.append(a)
-            w, ld_a, p = HOST, nx, a.ctypes.data
+            w, ld_a, p = HOST, a.strides[0] // 8, a.ctypes.data
         if where is None:
             where, ld = w, ld_a
         elif w != where or ld_a != ld:
@@ -194,7 +204,7 @@ class Solver:
         c = self.cfgs[member]
         if out is None:
             out = [np.empty((c.ny, c.nx), dtype=np.float64) for _ in range(6)]
-        p, ld, where, keep = _ptrs(out, c.nx, c.ny)
+        p, ld, where, keep = _ptrs(out, c.nx, c.ny, out=True)
         rc = lib().chimera_batch_get_state(self._h, member, *p, ld, where)
         if check:
             _check(rc, "get_state")
@@ -203,7 +213,7 @@ class Solver:
     def get_stage_buffer(self, b: int):
         c = self.cfgs[0]
         out = [np.empty((c.ny, c.nx), dtype=np.float64) for _ in range(6)]
-        p, ld, where, keep = _ptrs(out, c.nx, c.ny)
+        p, ld, where, keep = _ptrs(out, c.nx, c.ny, out=True)
         _check(lib().chimera_get_stage_buffer(self._h, b, *p, ld, where), "get_stage_buffer")
         return out
 
@@ -221,7 +231,7 @@ class Solver:
         if out is None:
             out = [np.empty((c.ny, c.nx), dtype=np.float64) for _ in range(6)]
         pi, ld_i, wi, keep_i = _ptrs(inputs, c.nx, c.ny)
-        po, ld_o, wo, keep_o = _ptrs(out, c.nx, c.ny)
+        po, ld_o, wo, keep_o = _ptrs(out, c.nx, c.ny, out=True)
         if wi != HOST or wo != HOST or ld_i != ld_o:
             raise ValueError("step_host takes host arrays with one pitch")
         P6 = C.c_void_p * 6

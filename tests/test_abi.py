@@ -103,3 +103,25 @@ def test_fortran_module_binds_every_entry_point_with_its_arity():
     assert sorted(set(c) - set(f)) == []
     assert sorted(set(f) - set(c)) == []
     assert {k: f[k] for k in c if f[k] != c[k]} == {}
+
+
+def test_host_arrays_pass_with_their_pitch():
+    """A view of a padded float64 host array goes to the library as it is
+    (pointer of the view, its row pitch as ld): an output written there lands
+    in the caller's array, not in a copy."""
+    import numpy as np
+    from chimera_b200.gpu import HOST, _ptrs
+    big = [np.zeros((9, 13)) for _ in range(6)]
+    views = [b[:8, :10] for b in big]
+    p, ld, where, _ = _ptrs(views, 10, 8, out=True)
+    assert ld == 13 and where == HOST
+    assert [x.value for x in p] == [v.ctypes.data for v in views]
+    dense = [np.zeros((8, 10)) for _ in range(6)]
+    assert _ptrs(dense, 10, 8, out=True)[1] == 10
+    # inputs that are not float64 / not x-contiguous are converted; outputs are refused
+    p, ld, _, keep = _ptrs([np.zeros((8, 10), dtype=np.float32)] * 6, 10, 8)
+    assert ld == 10 and keep[0].dtype == np.float64
+    with pytest.raises(ValueError):
+        _ptrs([np.zeros((8, 10), dtype=np.float32)] * 6, 10, 8, out=True)
+    with pytest.raises(ValueError):
+        _ptrs([b[:8, :20:2] for b in [np.zeros((8, 20))] * 6], 10, 8, out=True)
