@@ -18,6 +18,8 @@
 #include <tuple>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/chimera_gpu.h"
 #include "chimera_types.h"
 #include "kernel_table.h"
@@ -40,6 +42,17 @@ __global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__
 }
 
 bool valid_bc(int b) { return b >= CHIMERA_BC_PERIODIC && b <= CHIMERA_BC_INFLOW; }
+
+// NVTX range over the host-side span of an API call or a kernel launch: named
+// spans in a profiler's timeline (header-only NVTX; without a tool attached
+// each push / pop is a no-op).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+const char* const kLaunchName[4] = {"chimera cfl", "chimera stage 1", "chimera stage 2", "chimera stage 3"};
 
 // cuTensorMapEncodeTiled from the driver, through the runtime (the library
 // links only cudart); null if the driver does not provide it.
@@ -180,6 +193,7 @@ static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_b
 
 // kind: 0 = CFL kernel, 1..3 = stage kernels
 static int launch(chimera_handle* h, const KernelEntry& k, int grid, int kind) {
+  NvtxRange range(kLaunchName[kind]);
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(h->stream, &cs);
   if (!h->profiling || cs != cudaStreamCaptureStatusNone) return launch_raw(h, k, grid, 0, -1);
@@ -689,6 +703,7 @@ int chimera_get_stage_buffer(chimera_handle* h, int b, double* Mass, double* Mom
 // device-to-host copy overlaps the rest of stage 3.  Other handles take the
 // set_state / step / get_state sequence.
 int chimera_step_host(chimera_handle* h, const double* const* in, double* const* out, int ld) {
+  NvtxRange range("chimera_step_host");
   if (!h || !in || !out) return CHIMERA_ERR_BAD_ARG;
   const void* pi[6] = {in[0], in[1], in[2], in[3], in[4], in[5]};
   const void* po[6] = {out[0], out[1], out[2], out[3], out[4], out[5]};
@@ -772,6 +787,7 @@ int chimera_set_time(chimera_handle* h, double t, int output_count) {
 }
 
 int chimera_step(chimera_handle* h, int nsteps) {
+  NvtxRange range("chimera_step");
   if (!h || nsteps < 0) return CHIMERA_ERR_BAD_ARG;
   if (nsteps == 0) return CHIMERA_OK;
   return run_steps(h, nsteps);
@@ -785,6 +801,7 @@ int chimera_set_graph_steps(chimera_handle* h, int nsteps) {
 }
 
 int chimera_advance(chimera_handle* h, int max_steps, int* steps_taken) {
+  NvtxRange range("chimera_advance");
   if (!h || max_steps < 0) return CHIMERA_ERR_BAD_ARG;
   std::vector<Control> c(h->n);
   std::vector<unsigned long long> s0(h->n);
@@ -893,6 +910,7 @@ int chimera_set_variant(chimera_handle* h, int v) {
 }
 
 int chimera_autotune(chimera_handle* h, int reps, int* chosen, double* best_ms) {
+  NvtxRange range("chimera_autotune");
   if (!h || reps < 1) return CHIMERA_ERR_BAD_ARG;
   int rc = ensure_dt(h);
   if (rc) return rc;

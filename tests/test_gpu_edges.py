@@ -255,3 +255,36 @@ def test_canaries_around_no_alloc_arrays(G):
     for b, w in zip(bufs, ref.get_state()):
         assert np.array_equal(b[:n].cpu().numpy().reshape(cfg.ny, cfg.nx), w)
     ref.close()
+
+
+@pytest.mark.parametrize("case", ["4x4_periodic", "16x4_outflow", "5x7_mixed", "7x5_xoutflow"])
+def test_tiny_grids_fp32_every_variant(G, oracle, case):
+    """The FP32-bulk kernels (TMA variants included: their tiles fall back to
+    plain loads on grids smaller than a box) on tiny grids, against the FP64
+    oracle, with MOOD off: on these rough states the MC limiter often
+    saturates at exactly a neighbour's value, where the MOOD bound test is a
+    coin toss between two precisions (a single flip moves a 35-cell L1 by
+    1e-3).  Without MOOD, Rusanov + MC is continuous in the state (rounding
+    the start to FP32 moves the FP64 result by about 1e-8 here), so an L1
+    bound of 1e-5 per field after 6 steps separates FP32 arithmetic from an
+    indexing fault.  The MOOD indexing on tiny grids is checked bitwise in FP64
+    above."""
+    from chimera_b200.config import FP32_BULK
+    from tests.gpu_util import l1_rel
+    nx, ny, bc = TINY[case]
+    cfg, st = _state(nx, ny, bc, seed=nx * 17 + ny, riemann=RUSANOV)
+    cfg = cfg.replace(mood=False)
+    ref = oracle.State(st)
+    oracle.run(cfg, ref, 6)
+    s = G.Solver(cfg.replace(precision=FP32_BULK))
+    for v in range(s.variant_count()):
+        s.set_state(st)
+        s.set_time(0.0, 1)
+        s.set_variant(v)
+        s.step(6)
+        out = s.get_state()
+        for q in range(6):
+            err = l1_rel(out[q], ref.a[q])
+            assert err <= 1e-5, (case, v, q, err)
+        assert s.diag()["status"] == 0
+    s.close()
