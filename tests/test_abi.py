@@ -71,6 +71,14 @@ def test_null_arguments(lib):
     assert lib.chimera_create(None, None, C.byref(h)) == -1
     assert lib.chimera_step(None, 1) == -1
     assert lib.chimera_diag(None, None) == -1
+    P = C.c_void_p
+    # y-slab and dt hand-off entry points: a null handle is refused before any device call
+    assert lib.chimera_halo_pack(None, C.c_int(7), P(0), P(0)) == -1
+    assert lib.chimera_halo_unpack(None, C.c_int(7), P(0), P(0)) == -1
+    assert lib.chimera_slab_ghost_rows(None, C.c_int(7), C.c_int(7)) == -1
+    assert lib.chimera_refresh_dt(None, P(0)) == -1
+    assert lib.chimera_get_dt_device(None, P(0)) == -1
+    assert lib.chimera_set_dt_device(None, P(0)) == -1
     lib.chimera_destroy(None)
 
 
