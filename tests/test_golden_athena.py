@@ -9,7 +9,7 @@ import pytest
 
 from tests.golden import make_ot_athena as M
 
-SRC = "/root/reference/tests/validation/ot_reference.h5"
+SRC = M.DEFAULT_SRC   # the fixture script's source file (the reference checkout, where present)
 
 
 def test_fixture_shapes():
