@@ -27,6 +27,16 @@ namespace chimera {
 
 // Work-list / member descriptors (device side), see chimera_types.h.
 
+// A pointer read from global memory where it is used (inline PTX, so that the
+// compiler neither hoists the read nor merges it with an earlier one): keeps
+// the value out of registers through a phase that needs them all.  Only for
+// data no kernel writes (the member descriptors).
+__device__ __forceinline__ void* load_ptr(void* const* p) {
+  unsigned long long v;
+  asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return reinterpret_cast<void*>(v);
+}
+
 // Source cell of a (possibly out-of-domain) tile position: periodic wrap or
 // the nearest cell.  Positions of a ragged last tile can lie more than one
 // period beyond a small grid, so the wrap is a true modulo.
@@ -292,51 +302,47 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     const int sbuf = ctl->parity, obuf = 1 - sbuf;
     const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
     const int out_buf = (STAGE == 2) ? 2 : obuf;
-    const R* __restrict__ in[6];
-    const R* __restrict__ u0[6];
-    R* __restrict__ out[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
-      u0[q] = reinterpret_cast<const R*>(g.buf[sbuf][q]);
-      out[q] = reinterpret_cast<R*>(g.buf[out_buf][q]);
-    }
 
     // ---- phase 1: primitives on the tile + 2-cell halo ---------------------
     // average_face_to_cell_B (src/mhd_field_ops.f90:120-156) + get_primitive
     // (src/mhd_change_states.f90:61-113).  Out-of-domain positions take the
     // primitive of the cell that fill_ghost_cells would copy there
     // (src/mhd_bc.f90:36-121): wrap if periodic, else the nearest cell.
-    for (int p = tid; p < G::NP; p += NT) {
-      const int qx = p % G::PX, qy = p / G::PX;
-      const int si = map_index(i0 - 2 + qx, nx, px);
-      const int sj = map_index(j0 - 2 + qy, ny, py);
-      const size_t idx = size_t(sj) * nx + si;
-      const R bxc = in[4][idx];
-      const R byc = in[5][idx];
-      R Bx, By;
-      if (si > 0) Bx = R(0.5) * (bxc + in[4][idx - 1]);
-      else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
-      if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
-      else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
-      const R c0 = in[0][idx], c1 = in[1][idx], c2 = in[2][idx], c3 = in[3][idx];
-      if constexpr (KEEP_IN) {   // the tile's own cells: kept for phase 3b
-        const int ox = qx - 2, oy = qy - 2;
-        if (ox >= 0 && ox < TX && oy >= 0 && oy < TY) {
-          const int c = oy * TX + ox;
-          sU[0 * (TX * TY) + c] = c0;
-          sU[1 * (TX * TY) + c] = c1;
-          sU[2 * (TX * TY) + c] = c2;
-          sU[3 * (TX * TY) + c] = c3;
+    {
+      const R* __restrict__ in[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
+      for (int p = tid; p < G::NP; p += NT) {
+        const int qx = p % G::PX, qy = p / G::PX;
+        const int si = map_index(i0 - 2 + qx, nx, px);
+        const int sj = map_index(j0 - 2 + qy, ny, py);
+        const size_t idx = size_t(sj) * nx + si;
+        const R bxc = in[4][idx];
+        const R byc = in[5][idx];
+        R Bx, By;
+        if (si > 0) Bx = R(0.5) * (bxc + in[4][idx - 1]);
+        else Bx = px ? R(0.5) * (bxc + in[4][idx + (nx - 1)]) : bxc;
+        if (sj > 0) By = R(0.5) * (byc + in[5][idx - nx]);
+        else By = py ? R(0.5) * (byc + in[5][idx + size_t(ny - 1) * nx]) : byc;
+        const R c0 = in[0][idx], c1 = in[1][idx], c2 = in[2][idx], c3 = in[3][idx];
+        if constexpr (KEEP_IN) {   // the tile's own cells: kept for phase 3b
+          const int ox = qx - 2, oy = qy - 2;
+          if (ox >= 0 && ox < TX && oy >= 0 && oy < TY) {
+            const int c = oy * TX + ox;
+            sU[0 * (TX * TY) + c] = c0;
+            sU[1 * (TX * TY) + c] = c1;
+            sU[2 * (TX * TY) + c] = c2;
+            sU[3 * (TX * TY) + c] = c3;
+          }
         }
+        Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol);
+        sP[0 * G::NP + p] = pr.rho;
+        sP[1 * G::NP + p] = pr.vx;
+        sP[2 * G::NP + p] = pr.vy;
+        sP[3 * G::NP + p] = pr.P;
+        sP[4 * G::NP + p] = pr.Bx;
+        sP[5 * G::NP + p] = pr.By;
       }
-      Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol);
-      sP[0 * G::NP + p] = pr.rho;
-      sP[1 * G::NP + p] = pr.vx;
-      sP[2 * G::NP + p] = pr.vy;
-      sP[3 * G::NP + p] = pr.P;
-      sP[4 * G::NP + p] = pr.Bx;
-      sP[5 * G::NP + p] = pr.By;
     }
     __syncthreads();
 
@@ -424,6 +430,18 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
       if ((tid & 31) == 0 && s) atomicAdd(&ctl->mood_resets, (unsigned long long)s);
     }
     __syncthreads();
+
+    // the buffer pointers, read here rather than kept in registers through
+    // phase 2 (the kernel's register peak)
+    const R* __restrict__ in[6];
+    const R* __restrict__ u0[6];
+    R* __restrict__ out[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      in[q] = static_cast<const R*>(load_ptr(&g.buf[in_buf][q]));
+      u0[q] = static_cast<const R*>(load_ptr(&g.buf[sbuf][q]));
+      out[q] = static_cast<R*>(load_ptr(&g.buf[out_buf][q]));
+    }
 
     // ---- phase 3a: constrained transport -> new face B ------------------------
     // constrained_transport (src/mhd_flux.f90:79-136) + compute_curl_2d(-Ez)
