@@ -351,8 +351,12 @@ def run_chimera(args, world, rank, local):
     alg_bytes = STAGE_ACCESSES[kidx] * esize * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg[dom] * 1e-3) / 1e9
-    traffic = profile_traffic(f"{args.precision}_hlle_{dom}_rotor{n}")
-    inst_per_cell = profile_value("instructions", f"{args.precision}_hlle_{dom}_rotor{n}")
+    # the committed ncu figures of the tile variant this run uses (key suffix _v<variant>),
+    # else of the problem's profiled variant
+    pkey = f"{args.precision}_hlle_{dom}_rotor{n}"
+    vkey = f"{pkey}_v{s.variant()['variant']}"
+    traffic = profile_traffic(vkey) or profile_traffic(pkey)
+    inst_per_cell = profile_value("instructions", vkey) or profile_value("instructions", pkey)
 
     # --- end to end through the C-ABI with host buffers: every step copies the
     #     state in from pinned host memory, advances one step, copies it out.
