@@ -401,13 +401,20 @@ __device__ __forceinline__ int conserved_floors(R& M, R& Mx, R& My, R& E, R Bx, 
     E = hmax(E, (K<R>::P_floor / (gamma - R(1)) + halfB2) * vol);
     hit |= 1;
   }
-  R mag = dsqrt(Mx * Mx + My * My);
-  R v_mag = mag / M;
-  if (v_mag > R(50)) {
-    R scale = R(50) * M / mag;
-    Mx = Mx * scale;
-    My = My * scale;
-    hit |= 2;
+  // The velocity cap |Mom| / M > 50 can only apply where |Mom|^2 >= (40 M)^2:
+  // if the computed Mx^2 + My^2 < 1600 M^2, then |Mom| / M < 40 (1 + a few
+  // ulp), so the reference's test (square root, division, compare) would
+  // leave the cell alone -- skipping it there changes no bit.  NaN inputs fail
+  // the comparison and take the reference's path.
+  if (!(Mx * Mx + My * My < R(1600) * (M * M))) {
+    R mag = dsqrt(Mx * Mx + My * My);
+    R v_mag = mag / M;
+    if (v_mag > R(50)) {
+      R scale = R(50) * M / mag;
+      Mx = Mx * scale;
+      My = My * scale;
+      hit |= 2;
+    }
   }
   return hit;
 }
