@@ -213,3 +213,32 @@ def test_thermal_pressure_check_bitwise(O, ops):
     for k in slots:
         for x, y in zip(dev[k], ref[k]):
             _eq(x, y)
+
+
+def test_floor_velocity_cap_sweep(O, ops):
+    """The conserved floors' velocity cap (|Mom| / M > 50,
+    src/mhd_change_states.f90:116-166) for speeds across its threshold and
+    across 40, below which the GPU skips the reference's square root and
+    division (an exact pre-test): bit for bit against the oracle, including
+    the speeds 40 and 50 themselves and their neighbouring doubles."""
+    cfg, a = _state(O, BCS["periodic"])
+    ny, nx = a[0].shape
+    n = nx * ny
+    rng = np.random.default_rng(3)
+    special = [40.0, 50.0, np.nextafter(40.0, 0.0), np.nextafter(40.0, 99.0), np.nextafter(50.0, 0.0),
+               np.nextafter(50.0, 99.0), 39.999999999, 40.000000001, 49.9999999999, 50.0000000001, 1e3, 0.0]
+    speeds = np.concatenate([np.array(special), np.linspace(0.0, 100.0, n - len(special))])
+    rng.shuffle(speeds)
+    ang = rng.uniform(0.0, 2.0 * np.pi, n)
+    M = (0.5 + rng.random(n)) * cfg.dx * cfg.dy
+    Mx = (M * speeds * np.cos(ang)).reshape(ny, nx)
+    My = (M * speeds * np.sin(ang)).reshape(ny, nx)
+    M = M.reshape(ny, nx)
+    E = a[3].copy()
+    Bx, By = O.average_face_to_cell_B(cfg, a[4], a[5])
+    ref = O.apply_conserved_floors(cfg, M, Mx, My, E, Bx, By)
+    got = ops.apply_conserved_floors(cfg, *[_d(x) for x in (M, Mx, My, E, Bx, By)])
+    for x, y in zip(got, ref):
+        _eq(x, y)
+    capped = np.sqrt(ref[1] ** 2 + ref[2] ** 2) / ref[0]
+    assert np.sum(speeds > 50.0) > 100 and np.all(capped <= 50.0 * (1 + 1e-12))
