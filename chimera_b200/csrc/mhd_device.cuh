@@ -58,6 +58,11 @@ __device__ __forceinline__ float dcopysign(float a, float b) { return copysignf(
 __device__ __forceinline__ bool disfinite(double a) { return isfinite(a); }
 __device__ __forceinline__ bool disfinite(float a) { return isfinite(a); }
 
+// A running maximum: max(run, x) as fmax(run, x) gives it for a run that is
+// not NaN (a NaN x leaves run), as one compare and select -- FP64 fmax takes
+// several instructions on sm_100.
+__device__ __forceinline__ double run_max(double run, double x) { return (x > run) ? x : run; }
+
 // Primitive state of one cell: rho, vx, vy, P (TOTAL pressure), Bx, By.
 template <typename R> struct Prim {
   R rho, vx, vy, P, Bx, By;
@@ -107,8 +112,8 @@ __device__ __forceinline__ Prim<float> get_primitive_mixed(float M, float Mx, fl
   const double halfB2 = 0.5 * (bx * bx + by * by);
   const double ke = 0.5 * rd * (ud * ud + vd * vd);
   double P = ((double(E) * inv_vol - ke) - halfB2) * (gamma - 1.0) + halfB2;
-  P = fmax(P, 1.0e-12);
-  P = fmax(P, halfB2 + 1.0e-10 * (ke + halfB2));
+  P = run_max(1.0e-12, P);                              // = fmax(P, 1e-12), NaN included
+  P = run_max(P, halfB2 + 1.0e-10 * (ke + halfB2));      // P is not NaN here: = fmax
   p.rho = r; p.vx = u; p.vy = v; p.P = float(P); p.Bx = Bx; p.By = By;
   return p;
 }

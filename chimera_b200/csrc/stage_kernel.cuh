@@ -574,12 +574,12 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         const double By = hy ? 0.5 * (double(byn) + double(bym)) : double(byn);
         Prim<double> pr = get_primitive<double>(double(U[0]), double(U[1]), double(U[2]), double(U[3]),
                                                 Bx, By, g.gamma, g.vol);
-        e_speed = fmax(e_speed, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+        e_speed = run_max(e_speed, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
         const double d = fabs(divb_cell(double(bxn), double(bxm), double(byn), double(bym), hx, hy,
                                         g.inv_dx, g.inv_dy, g.square != 0));
-        e_dmax = fmax(e_dmax, d);
+        e_dmax = run_max(e_dmax, d);
         e_dsum += d;
-        e_bmax = fmax(e_bmax, sqrt(Bx * Bx + By * By));
+        e_bmax = run_max(e_bmax, sqrt(Bx * Bx + By * By));
         e_mass += double(U[0]);
         e_en += double(U[3]);
       }
@@ -642,18 +642,18 @@ __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
         const R By = hy ? R(0.5) * (byr + bymr) : byr;
         double spc, bm;
         speed_f32(in[0][k], in[1][k], in[2][k], in[3][k], Bx, By, g, spc, bm);
-        sp = fmax(sp, spc);
-        bmx = fmax(bmx, bm);
+        sp = run_max(sp, spc);
+        bmx = run_max(bmx, bm);
       } else {
         const double Bx = hx ? 0.5 * (bxc + bxm) : bxc;
         const double By = hy ? 0.5 * (byc + bym) : byc;
         Prim<double> pr = get_primitive<double>(double(in[0][k]), double(in[1][k]), double(in[2][k]),
                                                 double(in[3][k]), Bx, By, g.gamma, g.vol);
-        sp = fmax(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
-        bmx = fmax(bmx, sqrt(Bx * Bx + By * By));
+        sp = run_max(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+        bmx = run_max(bmx, sqrt(Bx * Bx + By * By));
       }
       const double d = fabs(divb_cell(bxc, bxm, byc, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
-      dmx = fmax(dmx, d);
+      dmx = run_max(dmx, d);
       dsum += d;
       ms += double(in[0][k]);
       es += double(in[3][k]);

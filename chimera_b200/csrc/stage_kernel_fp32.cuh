@@ -497,12 +497,12 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const R By = hy ? R(0.5) * (byn + bym) : byn;
         double spc, bm;
         speed_f32(U[0], U[1], U[2], U[3], Bx, By, g, spc, bm);
-        e_speed = fmax(e_speed, spc);
+        e_speed = run_max(e_speed, spc);
         const double dv = fabs(divb_cell(double(bxn), double(bxm), double(byn), double(bym), hx, hy,
                                          g.inv_dx, g.inv_dy, g.square != 0));
-        e_dmax = fmax(e_dmax, dv);
+        e_dmax = run_max(e_dmax, dv);
         e_dsum += dv;
-        e_bmax = fmax(e_bmax, bm);
+        e_bmax = run_max(e_bmax, bm);
         e_mass += double(U[0]);
         e_en += double(U[3]);
       }
