@@ -55,6 +55,24 @@ __device__ __forceinline__ float rk_blend(float u0, float u) {
   return (STAGE == 2) ? u0 + 0.25f * (u - u0) : u0 + (2.0f / 3.0f) * (u - u0);
 }
 
+// The MC limiter (apply_slope_limiter, src/mhd_derivatives.f90:86-96) on a
+// cell's x and y slopes at once: the adds and multiplies as sm_100's paired
+// FP32 instructions (two lanes each, round to nearest like the scalar ones),
+// the tests, absolute values and minima per lane -- the same bits as two
+// scalar limit_slope<float, LIMITER_MC> calls.
+__device__ __forceinline__ float2 limit_slope_mc2(float2 dfL, float2 dfR) {
+  const float2 prod = __fmul2_rn(dfL, dfR);
+  const float2 den = __fadd2_rn(dfL, dfR);
+  const float2 aL = __fmul2_rn(make_float2(2.0f, 2.0f), make_float2(fabsf(dfL.x), fabsf(dfL.y)));
+  const float2 aR = __fmul2_rn(make_float2(2.0f, 2.0f), make_float2(fabsf(dfR.x), fabsf(dfR.y)));
+  const float2 aD = __fmul2_rn(make_float2(0.5f, 0.5f), make_float2(fabsf(den.x), fabsf(den.y)));
+  const float2 m = make_float2(fminf(fminf(aL.x, aR.x), aD.x), fminf(fminf(aL.y, aR.y), aD.y));
+  float2 r = __fmul2_rn(make_float2(copysignf(1.0f, dfL.x), copysignf(1.0f, dfL.y)), m);
+  if (prod.x <= 0.0f || fabsf(den.x) < 1e-12f) r.x = 0.0f;
+  if (prod.y <= 0.0f || fabsf(den.y) < 1e-12f) r.y = 0.0f;
+  return r;
+}
+
 // Whether work item w's input box lies inside its member's arrays (and the
 // member has tensor maps): then it is loaded by TMA.
 template <int TX, int TY, int BW, int BH>
@@ -267,9 +285,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
           if (van_leer) {
             sx = limit_slope<R, LIMITER_VAN_LEER>((f0 - xm) * inv_dx, (xp - f0) * inv_dx);
             sy = limit_slope<R, LIMITER_VAN_LEER>((f0 - ym) * inv_dy, (yp - f0) * inv_dy);
-          } else {
-            sx = limit_slope<R, LIMITER_MC>((f0 - xm) * inv_dx, (xp - f0) * inv_dx);
-            sy = limit_slope<R, LIMITER_MC>((f0 - ym) * inv_dy, (yp - f0) * inv_dy);
+          } else {   // x and y lanes together (paired FP32 instructions)
+            const float2 inv = make_float2(inv_dx, inv_dy);
+            const float2 dfL = __fmul2_rn(__fadd2_rn(make_float2(f0, f0), make_float2(-xm, -ym)), inv);
+            const float2 dfR = __fmul2_rn(__fadd2_rn(make_float2(xp, yp), make_float2(-f0, -f0)), inv);
+            const float2 sl = limit_slope_mc2(dfL, dfR);
+            sx = sl.x;
+            sy = sl.y;
           }
         } else {
           sx = (xp - xm) * inv_2dx;
