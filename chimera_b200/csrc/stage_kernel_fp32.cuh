@@ -349,8 +349,12 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
           const R f0 = sP[q * G::NP + pa], fp = sP[q * G::NP + pb];
-          R vL = f0 + hh * sS[(2 * q + d) * G::NS + c];
-          R vR = fp - hh * sS[(2 * q + d) * G::NS + sb];
+          // left and right states as the two lanes of one paired FP32 multiply-add
+          const float2 v = __ffma2_rn(make_float2(hh, -hh),
+                                      make_float2(sS[(2 * q + d) * G::NS + c], sS[(2 * q + d) * G::NS + sb]),
+                                      make_float2(f0, fp));
+          R vL = v.x;
+          R vR = v.y;
           if (mood_on) {   // bounds of the LOW cell, reset to its value (src/mhd_derivatives.f90:213-216)
             if (vL < lo[q] || vL > hi[q]) { vL = f0; reset = true; }
             if (vR < lo[q] || vR > hi[q]) { vR = f0; reset = true; }
@@ -465,17 +469,25 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       const size_t idx = size_t(j) * nx + i;
       const int fxr = (lj + 1) * G::FXW + (li + 1);
       const int fyt = (lj + 1) * G::FYW + (li + 1);
+      // update_conserved (src/mhd_flux.f90:20-76), x pass then y pass, fields
+      // (0, 1) and (2, 3) as lanes of paired FP32 fused multiply-adds
       R U[4];
+      {
+        float2 F[2] = {make_float2(in[0][idx], in[1][idx]), make_float2(in[2][idx], in[3][idx])};
+        const float2 nax = make_float2(-ax, -ax), pax = make_float2(ax, ax);
+        const float2 nay = make_float2(-ay, -ay), pay = make_float2(ay, ay);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        R F = in[q][idx];
-        const R* fx = sFx + q * G::NFX;
-        const R* fy = sFy + q * G::NFY;
-        if (i > 0 || px) F = (F - ax * fx[fxr]) + ax * fx[fxr - 1];
-        else F = F - ax * fx[fxr];
-        if (j > 0 || py) F = (F - ay * fy[fyt]) + ay * fy[fyt - G::FYW];
-        else F = F - ay * fy[fyt];
-        U[q] = F;
+        for (int h = 0; h < 2; ++h) {
+          const R* fx0 = sFx + (2 * h) * G::NFX;
+          const R* fx1 = fx0 + G::NFX;
+          const R* fy0 = sFy + (2 * h) * G::NFY;
+          const R* fy1 = fy0 + G::NFY;
+          F[h] = __ffma2_rn(nax, make_float2(fx0[fxr], fx1[fxr]), F[h]);
+          if (i > 0 || px) F[h] = __ffma2_rn(pax, make_float2(fx0[fxr - 1], fx1[fxr - 1]), F[h]);
+          F[h] = __ffma2_rn(nay, make_float2(fy0[fyt], fy1[fyt]), F[h]);
+          if (j > 0 || py) F[h] = __ffma2_rn(pay, make_float2(fy0[fyt - G::FYW], fy1[fyt - G::FYW]), F[h]);
+        }
+        U[0] = F[0].x; U[1] = F[0].y; U[2] = F[1].x; U[3] = F[1].y;
       }
       const int pc = (lj + 2) * G::PX + (li + 2);
       const R cr = sP[0 * G::NP + pc], cu = sP[1 * G::NP + pc], cv = sP[2 * G::NP + pc];
@@ -497,9 +509,16 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         U[1] = U[1] + ay * (cr * cv * cu - cBy * cBx);
         U[3] = U[3] + ay * ((en + cP) * cv - cBy * (cBy * cv + cBx * cu));
       }
-      if (STAGE >= 2) {
+      if (STAGE >= 2) {   // rk_blend, fields in pairs: u0 + c (u - u0)
+        const float c = (STAGE == 2) ? 0.25f : (2.0f / 3.0f);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) U[q] = rk_blend<STAGE>(u0[q][idx], U[q]);
+        for (int h = 0; h < 2; ++h) {
+          const float2 a0 = make_float2(u0[2 * h][idx], u0[2 * h + 1][idx]);
+          const float2 d = __fadd2_rn(make_float2(U[2 * h], U[2 * h + 1]), make_float2(-a0.x, -a0.y));
+          const float2 r = __ffma2_rn(make_float2(c, c), d, a0);
+          U[2 * h] = r.x;
+          U[2 * h + 1] = r.y;
+        }
       }
       if (STAGE >= 2) floor_hits += conserved_floors<R>(U[0], U[1], U[2], U[3], cBx, cBy, gamma, vol) ? 1u : 0u;
 #pragma unroll
