@@ -73,6 +73,57 @@ __device__ __forceinline__ float2 limit_slope_mc2(float2 dfL, float2 dfR) {
   return r;
 }
 
+// rusanov_flux (src/mhd_flux.f90:197-288) in FP32, the same expressions as
+// rusanov<float>, with the left and right states' identical work (magnetic,
+// thermal and kinetic terms, total energy, fast speed) and the five flux
+// corrections as lanes of sm_100's paired FP32 instructions.
+__device__ __forceinline__ Flux5<float> rusanov_x2(float gamma, float rho_L, float rho_R, float vx_L, float vx_R,
+                                                   float vy_L, float vy_R, float P_L, float P_R, float Bx_L,
+                                                   float Bx_R, float By_L, float By_R) {
+  const float2 half = make_float2(0.5f, 0.5f);
+  const float2 rho = make_float2(rho_L, rho_R), vx = make_float2(vx_L, vx_R), vy = make_float2(vy_L, vy_R);
+  const float2 Bx = make_float2(Bx_L, Bx_R), By = make_float2(By_L, By_R);
+  const float2 halfB2 = __fmul2_rn(half, __ffma2_rn(Bx, Bx, __fmul2_rn(By, By)));
+  float2 p_th = __fadd2_rn(make_float2(P_L, P_R), make_float2(-halfB2.x, -halfB2.y));
+  p_th.x = fmaxf(p_th.x, 1.0e-12f);
+  p_th.y = fmaxf(p_th.y, 1.0e-12f);
+  const float gm1 = gamma - 1.0f;
+  const float igm1 = 1.0f / gm1;
+  const float2 ke = __fmul2_rn(__fmul2_rn(half, rho), __ffma2_rn(vx, vx, __fmul2_rn(vy, vy)));
+  const float2 en = __fadd2_rn(__ffma2_rn(p_th, make_float2(igm1, igm1), ke), halfB2);
+  const float2 mx = __fmul2_rn(rho, vx), my = __fmul2_rn(rho, vy);
+  const float rho_avg = 0.5f * (rho_L + rho_R);
+  const float inv_rho_avg = 1.0f / rho_avg;
+  const float momx_avg = 0.5f * (mx.x + mx.y);
+  const float momy_avg = 0.5f * (my.x + my.y);
+  const float en_avg = 0.5f * (en.x + en.y);
+  const float Bx_avg = 0.5f * (Bx_L + Bx_R);
+  const float By_avg = 0.5f * (By_L + By_R);
+  const float hB = 0.5f * (Bx_avg * Bx_avg + By_avg * By_avg);
+  const float P_avg = gm1 * ((en_avg - 0.5f * (momx_avg * momx_avg + momy_avg * momy_avg) * inv_rho_avg) - hB) + hB;
+  Flux5<float> F;
+  F.mass = momx_avg;
+  F.momn = (momx_avg * momx_avg * inv_rho_avg + P_avg) - Bx_avg * Bx_avg;
+  F.momt = momx_avg * momy_avg * inv_rho_avg - Bx_avg * By_avg;
+  F.energy = (en_avg + P_avg) * momx_avg * inv_rho_avg -
+             Bx_avg * (Bx_avg * momx_avg + By_avg * momy_avg) * inv_rho_avg;
+  F.bt = (By_avg * momx_avg - Bx_avg * momy_avg) * inv_rho_avg;
+  // c^2 = (gamma p_th + B^2) / rho > 0 (the thermal pressure is floored)
+  const float2 c2 = __fmul2_rn(__ffma2_rn(make_float2(gamma, gamma), p_th, __fmul2_rn(make_float2(2.0f, 2.0f), halfB2)),
+                               make_float2(1.0f / rho_L, 1.0f / rho_R));
+  const float2 h = __fmul2_rn(half, __fadd2_rn(c2, make_float2(fabsf(c2.x), fabsf(c2.y))));
+  const float2 Cs = __fadd2_rn(make_float2(sqrtf(h.x), sqrtf(h.y)), make_float2(fabsf(vx_L), fabsf(vx_R)));
+  const float C = 0.5f * fmaxf(Cs.x, Cs.y);
+  const float2 nC = make_float2(-C, -C);
+  const float2 f01 = __ffma2_rn(nC, __fadd2_rn(make_float2(rho_R, mx.y), make_float2(-rho_L, -mx.x)),
+                                make_float2(F.mass, F.momn));
+  const float2 f23 = __ffma2_rn(nC, __fadd2_rn(make_float2(my.y, en.y), make_float2(-my.x, -en.x)),
+                                make_float2(F.momt, F.energy));
+  F.mass = f01.x; F.momn = f01.y; F.momt = f23.x; F.energy = f23.y;
+  F.bt = F.bt - C * (By_R - By_L);
+  return F;
+}
+
 // Whether work item w's input box lies inside its member's arrays (and the
 // member has tensor maps): then it is loaded by TMA.
 template <int TX, int TY, int BW, int BH>
@@ -378,7 +429,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const R utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
         const R bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
         const R btL = ydir ? L[4] : L[5], btR = ydir ? Rv[4] : Rv[5];
-        Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
+        Flux5<R> F;
+        if constexpr (SOLVER == RIEMANN_RUSANOV)
+          F = rusanov_x2(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
+        else
+          F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
         R* dst = ydir ? sFy : sFx;
         const int NF = ydir ? G::NFY : G::NFX;
         dst[0 * NF + ff] = F.mass;
