@@ -106,8 +106,10 @@ __device__ __forceinline__ Prim<float> get_primitive_mixed(float M, float Mx, fl
   Prim<float> p;
   const float r = fmaxf(M * inv_volf, 1.0e-12f);
   const float ir = 1.0f / r;
-  const float u = (Mx * inv_volf) * ir;
-  const float v = (My * inv_volf) * ir;
+  // u and v as the two lanes of paired FP32 multiplies (the same bits as scalar ones)
+  const float2 uv = __fmul2_rn(__fmul2_rn(make_float2(Mx, My), make_float2(inv_volf, inv_volf)), make_float2(ir, ir));
+  const float u = uv.x;
+  const float v = uv.y;
   const double rd = r, ud = u, vd = v, bx = Bx, by = By;
   const double halfB2 = 0.5 * (bx * bx + by * by);
   const double ke = 0.5 * rd * (ud * ud + vd * vd);

@@ -466,14 +466,22 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
     // ---- phase 3a: constrained transport -> new face B ----------------------------
     const R* FByX = sFx + 4 * G::NFX;
     const R* FBxY = sFy + 4 * G::NFY;
-    auto Ez = [&](int ci, int cj) -> R {
-      const int xi = (cj - j0 + 1) * G::FXW + (ci - i0 + 1);
-      const R fa = FByX[xi];
-      const R up = (cj == ny - 1 && !py) ? fa : FByX[xi + G::FXW];
-      const int yi = (cj - j0 + 1) * G::FYW + (ci - i0 + 1);
-      const R fb = FBxY[yi];
-      const R right = (ci == nx - 1 && !px) ? fb : FBxY[yi + 1];
-      return R(0.25) * (((-fa - up) + fb) + right);
+    // corner Ez (src/mhd_flux.f90:79-136) at two corners, as the lanes of paired FP32 adds and a
+    // multiply: 0.25 (((-FByX(i,j) - FByX(i,j+1)) + FBxY(i,j)) + FBxY(i+1,j)), zero-gradient at
+    // non-periodic top / right
+    auto Ez2 = [&](int ci0, int cj0, int ci1, int cj1) -> float2 {
+      const int xi0 = (cj0 - j0 + 1) * G::FXW + (ci0 - i0 + 1), xi1 = (cj1 - j0 + 1) * G::FXW + (ci1 - i0 + 1);
+      const int yi0 = (cj0 - j0 + 1) * G::FYW + (ci0 - i0 + 1), yi1 = (cj1 - j0 + 1) * G::FYW + (ci1 - i0 + 1);
+      const R fa0 = FByX[xi0], fa1 = FByX[xi1];
+      const R up0 = (cj0 == ny - 1 && !py) ? fa0 : FByX[xi0 + G::FXW];
+      const R up1 = (cj1 == ny - 1 && !py) ? fa1 : FByX[xi1 + G::FXW];
+      const R fb0 = FBxY[yi0], fb1 = FBxY[yi1];
+      const R rt0 = (ci0 == nx - 1 && !px) ? fb0 : FBxY[yi0 + 1];
+      const R rt1 = (ci1 == nx - 1 && !px) ? fb1 : FBxY[yi1 + 1];
+      float2 t = __fadd2_rn(make_float2(-fa0, -fa1), make_float2(-up0, -up1));
+      t = __fadd2_rn(t, make_float2(fb0, fb1));
+      t = __fadd2_rn(t, make_float2(rt0, rt1));
+      return __fmul2_rn(make_float2(0.25f, 0.25f), t);
     };
     const int bx_lo = (STAGE == 3 && (i0 > 0 || px)) ? -1 : 0;
     const int by_lo = (STAGE == 3 && (j0 > 0 || py)) ? -1 : 0;
@@ -491,19 +499,17 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       const size_t idx = size_t(gj) * nx + gi;
       R val;
       if (!isy) {
-        const R e0 = Ez(i, j);
-        R dbx;
-        if (j > 0 || py) dbx = ((-e0) - (-Ez(i, j - 1))) * inv_dy;
-        else dbx = ((-Ez(i, 1)) - (-e0)) * inv_dy;
+        const bool inner = j > 0 || py;
+        const float2 e = Ez2(i, j, i, inner ? j - 1 : 1);
+        const R dbx = inner ? ((-e.x) - (-e.y)) * inv_dy : ((-e.y) - (-e.x)) * inv_dy;   // outflow ylo: copy row 2
         val = in[4][idx] + dt * dbx;
         if (STAGE >= 2) val = rk_blend<STAGE>(u0[4][idx], val);
         if (STAGE == 3) sBx[lj * G::BXW + (li + 1)] = val;   // the epilogue reads neighbours' new B
         else out[4][idx] = val;                                // stages 1, 2: straight to the output
       } else {
-        const R e0 = Ez(i, j);
-        R dby;
-        if (i > 0 || px) dby = -(((-e0) - (-Ez(i - 1, j))) * inv_dx);
-        else dby = -(((-Ez(1, j)) - (-e0)) * inv_dx);
+        const bool inner = i > 0 || px;
+        const float2 e = Ez2(i, j, inner ? i - 1 : 1, j);
+        const R dby = inner ? -(((-e.x) - (-e.y)) * inv_dx) : -(((-e.y) - (-e.x)) * inv_dx);   // outflow xlo: copy column 2
         val = in[5][idx] + dt * dby;
         if (STAGE >= 2) val = rk_blend<STAGE>(u0[5][idx], val);
         if (STAGE == 3) sBy[(lj + 1) * G::BYW + li] = val;
