@@ -649,12 +649,16 @@ int chimera_batch_set_state(chimera_handle* h, int m, const double* Mass, const 
   Control c;
   rc = read_ctl(h, m, &c);
   if (rc) return rc;
-  for (int q = 0; q < 6; ++q) {
+  for (int q = 0; q < 6 && !rc; ++q)
     rc = copy_field_in(h, m, h->hm[m].buf[c.parity][q], (const double*)ptrs[q], ld, where);
-    if (rc) return rc;
-  }
   h->dt_valid[m] = false;
-  return CHIMERA_OK;
+  // Host arrays have been read completely when the call returns: copies from
+  // page-locked memory would otherwise still be in flight.
+  if (where == CHIMERA_HOST) {
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e);
+  }
+  return rc;
 }
 
 int chimera_set_state(chimera_handle* h, const double* Mass, const double* Momx, const double* Momy,
@@ -670,11 +674,10 @@ static int get_buffer(chimera_handle* h, int m, int which, double* const* ptrs, 
   rc = read_ctl(h, m, &c);
   if (rc) return rc;
   const int b = (which == 0) ? c.parity : (which == 1 ? 1 - c.parity : 2);
-  for (int q = 0; q < 6; ++q) {
-    rc = copy_field_out(h, m, ptrs[q], h->hm[m].buf[b][q], ld, where);
-    if (rc) return rc;
-  }
-  CK(cudaStreamSynchronize(h->stream));
+  for (int q = 0; q < 6 && !rc; ++q) rc = copy_field_out(h, m, ptrs[q], h->hm[m].buf[b][q], ld, where);
+  const cudaError_t e = cudaStreamSynchronize(h->stream);   // on the error path too: no copy outlives the call
+  if (rc) { cudaGetLastError(); return rc; }
+  if (e != cudaSuccess) return cuda_fail(e);
   return c.status ? CHIMERA_ERR_NONFINITE : CHIMERA_OK;
 }
 
@@ -721,48 +724,59 @@ int chimera_step_host(chimera_handle* h, const double* const* in, double* const*
   if (rc) return rc;
   const chimera_cfg& cf = h->cfg[0];
   const Member& g = h->hm[0];
-  for (int q = 0; q < 6; ++q) {
-    rc = copy_field_in(h, 0, g.buf[c.parity][q], in[q], ld, CHIMERA_HOST);
-    if (rc) return rc;
-  }
   h->dt_valid[0] = false;
-  if (!c.active) {   // t >= t_end: no step is taken, the state goes back unchanged
+  // Everything issued here is asynchronous, on the handle's stream and the
+  // copy stream; the exit below drains both, so that no copy from in[] or into
+  // out[] outlives the call, on the error paths too.
+  auto issue = [&]() -> int {
     for (int q = 0; q < 6; ++q) {
-      rc = copy_field_out(h, 0, out[q], g.buf[c.parity][q], ld, CHIMERA_HOST);
-      if (rc) return rc;
+      const int e = copy_field_in(h, 0, g.buf[c.parity][q], in[q], ld, CHIMERA_HOST);
+      if (e) return e;
     }
-    CK(cudaStreamSynchronize(h->stream));
+    if (!c.active) {   // t >= t_end: no step is taken, the state goes back unchanged
+      for (int q = 0; q < 6; ++q) {
+        const int e = copy_field_out(h, 0, out[q], g.buf[c.parity][q], ld, CHIMERA_HOST);
+        if (e) return e;
+      }
+      return CHIMERA_OK;
+    }
+    int e = ensure_dt(h);
+    for (int s = 0; s < 2 && !e; ++s) e = launch(h, h->ks.stage[h->riemann - 1][s], h->grid_stage[s], s + 1);
+    if (e) return e;
+    if (!h->copy_stream) {
+      CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+      for (auto& ev : h->band_done) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    // bands of tile rows (work items are row-major within the grid)
+    const int ty = h->ks.stage[0][0].ty;
+    const int rows = g.tiles_y, nb = std::min(rows, int(sizeof(h->band_done) / sizeof(h->band_done[0])));
+    const int out_buf = 1 - c.parity;   // stage 3 writes U^{n+1} there; the finish flips the parity
+    const KernelEntry& k3 = h->ks.stage[h->riemann - 1][2];
+    for (int b = 0; b < nb; ++b) {
+      const int r0 = rows * b / nb, r1 = rows * (b + 1) / nb;
+      const int w0 = r0 * g.tiles_x, w1 = r1 * g.tiles_x;
+      const int grid = std::max(1, std::min(h->grid_stage[2], w1 - w0));
+      e = launch_raw(h, k3, grid, w0, w1);
+      if (e) return e;
+      CK(cudaEventRecord(h->band_done[b], h->stream));
+      CK(cudaStreamWaitEvent(h->copy_stream, h->band_done[b], 0));
+      const int y0 = r0 * ty, y1 = std::min(r1 * ty, cf.ny);
+      const size_t w = size_t(cf.nx) * sizeof(double);
+      for (int q = 0; q < 6; ++q)
+        CK(cudaMemcpy2DAsync(out[q] + size_t(y0) * ld, size_t(ld) * sizeof(double),
+                             static_cast<const char*>(g.buf[out_buf][q]) + size_t(y0) * w, w, w, y1 - y0,
+                             cudaMemcpyDeviceToHost, h->copy_stream));
+    }
     return CHIMERA_OK;
-  }
-  rc = ensure_dt(h);
-  for (int s = 0; s < 2 && !rc; ++s) rc = launch(h, h->ks.stage[h->riemann - 1][s], h->grid_stage[s], s + 1);
-  if (rc) return rc;
-  if (!h->copy_stream) {
-    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-    for (auto& e : h->band_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  }
-  // bands of tile rows (work items are row-major within the grid)
-  const int ty = h->ks.stage[0][0].ty;
-  const int rows = g.tiles_y, nb = std::min(rows, int(sizeof(h->band_done) / sizeof(h->band_done[0])));
-  const int out_buf = 1 - c.parity;   // stage 3 writes U^{n+1} there; the finish flips the parity
-  const KernelEntry& k3 = h->ks.stage[h->riemann - 1][2];
-  for (int b = 0; b < nb; ++b) {
-    const int r0 = rows * b / nb, r1 = rows * (b + 1) / nb;
-    const int w0 = r0 * g.tiles_x, w1 = r1 * g.tiles_x;
-    const int grid = std::max(1, std::min(h->grid_stage[2], w1 - w0));
-    rc = launch_raw(h, k3, grid, w0, w1);
-    if (rc) return rc;
-    CK(cudaEventRecord(h->band_done[b], h->stream));
-    CK(cudaStreamWaitEvent(h->copy_stream, h->band_done[b], 0));
-    const int y0 = r0 * ty, y1 = std::min(r1 * ty, cf.ny);
-    const size_t w = size_t(cf.nx) * sizeof(double);
-    for (int q = 0; q < 6; ++q)
-      CK(cudaMemcpy2DAsync(out[q] + size_t(y0) * ld, size_t(ld) * sizeof(double),
-                           static_cast<const char*>(g.buf[out_buf][q]) + size_t(y0) * w, w, w, y1 - y0,
-                           cudaMemcpyDeviceToHost, h->copy_stream));
-  }
+  };
+  rc = issue();
+  const cudaError_t e_copy = h->copy_stream ? cudaStreamSynchronize(h->copy_stream) : cudaSuccess;
+  const cudaError_t e_main = cudaStreamSynchronize(h->stream);
+  if (rc) { cudaGetLastError(); return rc; }
+  if (e_copy != cudaSuccess) return cuda_fail(e_copy);
+  if (e_main != cudaSuccess) return cuda_fail(e_main);
+  if (!c.active) return CHIMERA_OK;
   h->dt_valid[0] = true;   // the stage-3 finish computed the next dt
-  CK(cudaStreamSynchronize(h->copy_stream));
   rc = read_ctl(h, 0, &c);
   if (rc) return rc;
   return c.status ? CHIMERA_ERR_NONFINITE : CHIMERA_OK;

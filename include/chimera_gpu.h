@@ -95,7 +95,9 @@ typedef struct chimera_handle chimera_handle;
  * Replaces the allocations of src/mhd_init.f90:99-164 for the path's arrays. */
 int chimera_create(const chimera_cfg* cfg, void* stream, chimera_handle** out);
 
-/* Copy a conserved state in (host or device arrays); marks dt stale.
+/* Copy a conserved state in (host or device arrays); marks dt stale.  Host
+ * arrays have been read completely when the call returns (it synchronises);
+ * device arrays are read in order on the handle's stream.
  * Replaces the module globals Mass..b_y (src/mhd_init.f90:44-47). */
 int chimera_set_state(chimera_handle* h, const double* Mass, const double* Momx,
                       const double* Momy, const double* Energy, const double* b_x,

@@ -88,3 +88,26 @@ def test_step_host_fp32_handle(G):
         out = s.step_host(out)
         for q in range(6):
             assert np.array_equal(out[q], ref[k][0][q])
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_set_state_has_read_pinned_arrays_on_return(G, fp32):
+    """set_state from page-locked host tensors: the caller may overwrite them
+    as soon as the call returns (host arrays are read completely before it
+    returns), and get_state gives back exactly what was set."""
+    cfg, st = P.rotor(1024)   # 48 MB of state: a copy still in flight would be seen
+    if fp32:
+        cfg = cfg.replace(precision=FP32_BULK)
+    s = G.Solver(cfg)
+    pinned = _pinned(st)
+    s.set_state(pinned)
+    for t in pinned:
+        t.fill_(float("nan"))
+    got = s.get_state()
+    ref = G.Solver(cfg)       # the same arrays set from pageable numpy memory
+    ref.set_state(st)
+    want = ref.get_state()    # FP32-bulk: the set values rounded to FP32
+    ref.close()
+    s.close()
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
