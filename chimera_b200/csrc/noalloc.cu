@@ -44,6 +44,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_addr[NA_MAX_DEVICES] = {nullptr};
+// One call at a time per device within this process: a call holds its
+// device's lock from the first launch to the final stream synchronisation, so
+// host threads cannot interleave their use of the one scratch array.
+std::mutex g_call_mutex[NA_MAX_DEVICES];
 
 // Per-call set-up of the descriptors inside the scratch.  Control must start
 // at zero (tiles_done counts finished tiles); everything else in the scratch is
@@ -59,7 +63,7 @@ __global__ void k_noalloc_init(Member* m, Control* c, Member desc, double t, int
   }
 }
 
-int scratch_for_current_device(unsigned char** out) {
+int scratch_for_current_device(unsigned char** out, int* device) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) {
     cudaGetLastError();
@@ -76,6 +80,7 @@ int scratch_for_current_device(unsigned char** out) {
     g_scratch_addr[dev] = static_cast<unsigned char*>(p);
   }
   *out = g_scratch_addr[dev];
+  *device = dev;
   return CHIMERA_OK;
 }
 
@@ -100,8 +105,10 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   if (cells > NA_MAX_CELLS) return CHIMERA_ERR_TOO_LARGE;
 
   unsigned char* base = nullptr;
-  int rc = scratch_for_current_device(&base);
+  int dev = -1;
+  int rc = scratch_for_current_device(&base, &dev);
   if (rc) return rc;
+  std::lock_guard<std::mutex> call_lock(g_call_mutex[dev]);
   cudaStream_t s = (cudaStream_t)stream;
 
   Member g;
@@ -147,8 +154,8 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   a.counters = 0;
   a.dry = 0;
 
-  k_noalloc_init<<<1, 32, 0, s>>>(d_member, d_ctl, g, *t, *output_count);
   if (size_t(a.total_tiles) > NA_MAX_TILES) return CHIMERA_ERR_TOO_LARGE;
+  k_noalloc_init<<<1, 32, 0, s>>>(d_member, d_ctl, g, *t, *output_count);
   const int grid = a.total_tiles;
   const size_t smem = TileGeom<NA_TX, NA_TY>::smem_bytes<double>();
   cfl_kernel<double, NA_TX, NA_TY, NA_NT><<<grid, NA_NT, 0, s>>>(a);

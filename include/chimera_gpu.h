@@ -266,8 +266,10 @@ void chimera_adjoint_destroy(chimera_adjoint* a);
  *     the dt the next step will take.  The call synchronises the stream.
  *   - The first call on a device looks up the scratch's device address; make
  *     that first call before any stream capture.
- *   - Every call shares the one scratch array: calls that overlap on the GPU
- *     (other host threads, other streams) race and must be serialised. */
+ *   - Every call shares the one scratch array of its device.  Calls from
+ *     several host threads of one process are serialised per device inside
+ *     the library; calls from other processes use their own copy.  A call
+ *     made during a stream capture is not supported (it synchronises). */
 #define CHIMERA_NOALLOC_MAX_CELLS 65536
 int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, double* Momx, double* Momy,
                              double* Energy, double* b_x, double* b_y, double* t,

@@ -74,3 +74,65 @@ def test_noalloc_rejects_oversize_and_bad_args():
     fp32 = G.to_ccfg(P.orszag_tang(8)[0].replace(precision=1))
     assert step(C.byref(fp32), *([ptr] * 6), C.byref(t), C.byref(oc), None, None) == -5
     assert step(None, *([ptr] * 6), C.byref(t), C.byref(oc), None, None) == -1
+
+
+def test_noalloc_two_host_threads_are_serialised():
+    """Two host threads, each on its own CUDA stream, step their own grids
+    through the one scratch array at the same time: each must get the handle
+    path's bits.  Both grids have one shape (different states), so every
+    access stays inside the arrays whatever the interleaving."""
+    import threading
+
+    import torch
+    G = require_gpu()
+    step = _noalloc(G)
+    cfg, st0 = P.rotor(64, riemann=HLLE)
+    h = G.Solver(cfg)
+    h.set_state(st0)
+    h.step(1)
+    st1 = h.get_state()
+    h.close()
+    states, wants = [st0, st1], []
+    for st in states:
+        r = G.Solver(cfg)
+        r.set_state(st)
+        outs = []
+        for _ in range(4):
+            r.step(1)
+            outs.append(r.get_state())
+        wants.append(outs)
+        r.close()
+    ccfg = G.to_ccfg(cfg)
+    results, errors = [None, None], []
+    start = threading.Barrier(2)
+
+    def worker(k):
+        try:
+            s = torch.cuda.Stream()
+            dev = [torch.from_numpy(a.copy()).cuda() for a in states[k]]
+            torch.cuda.synchronize()
+            t, oc, dtn = C.c_double(0.0), C.c_int(1), C.c_double(0.0)
+            got = []
+            start.wait(timeout=60)
+            for _ in range(4):
+                rc = step(C.byref(ccfg), *[C.c_void_p(x.data_ptr()) for x in dev], C.byref(t), C.byref(oc),
+                          C.byref(dtn), C.c_void_p(s.cuda_stream))
+                if rc:
+                    errors.append((k, rc))
+                    return
+                got.append([x.cpu().numpy() for x in dev])
+            results[k] = got
+        except Exception as e:   # reported below, on the main thread
+            errors.append((k, e))
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join(timeout=120)
+    assert not errors, errors
+    for k in range(2):
+        assert results[k] is not None
+        for call in range(4):
+            for q in range(6):
+                assert np.array_equal(results[k][call][q], wants[k][call][q]), (k, call, q)
