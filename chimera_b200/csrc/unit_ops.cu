@@ -25,6 +25,10 @@ struct OpGeom {
 
 int make_geom(const chimera_cfg* c, OpGeom* g) {
   if (!c || c->nx < 2 || c->ny < 2 || !(c->dx > 0) || !(c->dy > 0)) return CHIMERA_ERR_BAD_ARG;
+  for (int side : {c->bc_xlo, c->bc_xhi, c->bc_ylo, c->bc_yhi})
+    if (side < CHIMERA_BC_PERIODIC || side > CHIMERA_BC_INFLOW) return CHIMERA_ERR_BAD_ARG;
+  // the kernels index the (nx + 2) x (ny + 2) padded arrays with int
+  if ((long long)(c->nx + 2) * (c->ny + 2) > 0x7fffffffLL) return CHIMERA_ERR_TOO_LARGE;
   g->nx = c->nx; g->ny = c->ny;
   g->xlo = c->bc_xlo == CHIMERA_BC_PERIODIC; g->xhi = c->bc_xhi == CHIMERA_BC_PERIODIC;
   g->ylo = c->bc_ylo == CHIMERA_BC_PERIODIC; g->yhi = c->bc_yhi == CHIMERA_BC_PERIODIC;

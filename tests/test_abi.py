@@ -133,3 +133,22 @@ def test_host_arrays_pass_with_their_pitch():
         _ptrs([np.zeros((8, 10), dtype=np.float32)] * 6, 10, 8, out=True)
     with pytest.raises(ValueError):
         _ptrs([b[:8, :20:2] for b in [np.zeros((8, 20))] * 6], 10, 8, out=True)
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(nx=1), -1),
+    (dict(dy=0.0), -1),
+    (dict(riemann=4), -1),
+    (dict(bc=(1, 1, 5, 5)), -1),         # side values are 1..4 (src/mhd_config.f90:40-43)
+    (dict(nx=50000, ny=50000), -8),      # (nx + 2)(ny + 2) beyond the kernels' int indices
+])
+def test_unit_ops_reject_bad_config(lib, kw, code):
+    """The per-routine entry points check cfg before any device call (the
+    pointers below are never dereferenced: each call returns first)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the refusal without a device")
+    cfg = _cfg(**kw)
+    P = C.c_void_p
+    assert lib.chimera_op_average_face_to_cell_B(C.byref(cfg), P(8), P(8), P(8), P(8), None) == code
+    assert lib.chimera_op_compute_divB(C.byref(cfg), P(8), P(8), P(8), None) == code
