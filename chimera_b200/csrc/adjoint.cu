@@ -528,6 +528,7 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
       cfg->bc_ylo != CHIMERA_BC_PERIODIC || cfg->bc_yhi != CHIMERA_BC_PERIODIC)
     return CHIMERA_ERR_UNSUPPORTED;
   if (cfg->precision != CHIMERA_FP64) return CHIMERA_ERR_UNSUPPORTED;
+  if ((long long)cfg->nx * cfg->ny >= (1LL << 31)) return CHIMERA_ERR_TOO_LARGE;   // int cell indices
   chimera_adjoint* a = new (std::nothrow) chimera_adjoint();
   if (!a) return CHIMERA_ERR_NOMEM;
   AdjGeom& g = a->g;
@@ -547,8 +548,12 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
     if (cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking) != cudaSuccess) { delete a; return adj_fail(); }
     a->own_stream = true;
   }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+  }
   a->grid = sms * 8;
   // doubles per cell: tapes 3 x (6 P + 10 F + 4 Upre + 4 Ublend) + 2 flag words (as 1 double)
   // + reverse (4 + 2 + 2 + 1 + 48 + 24 + 6 + 2) + U1, U2, lA, lB, lU0 (30)
