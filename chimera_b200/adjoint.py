@@ -71,6 +71,13 @@ class Adjoint:
         except Exception:
             pass
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
     def forward_step(self, U, dt):
         out = [torch.empty_like(u) for u in U]
         rc = _lib().chimera_adjoint_forward_step(self._h, _ptr6(U), float(dt), _ptr6(out))
@@ -89,13 +96,12 @@ class Adjoint:
 def cfl_dts(cfg: SolverConfig, U, nsteps: int):
     """The dt sequence of an FP64 primal run from U (the CFL dt with the tOut
     clip of every step), through the fused solver."""
-    s = gpu.Solver(cfg.replace(precision=FP64))
-    s.set_state([u.contiguous() for u in U])
     dts = []
-    for _ in range(nsteps):
-        dts.append(s.diag()["dt"])
-        s.step(1)
-    s.close()
+    with gpu.Solver(cfg.replace(precision=FP64)) as s:
+        s.set_state([u.contiguous() for u in U])
+        for _ in range(nsteps):
+            dts.append(s.diag()["dt"])
+            s.step(1)
     return dts
 
 

@@ -32,8 +32,12 @@ def make_batch(cfgs, states, gpu_module=None):
     if gpu_module is None:
         from . import gpu as gpu_module
     s = gpu_module.Solver(cfgs)
-    for m, st in enumerate(states):
-        s.set_state(st, member=m)
+    try:
+        for m, st in enumerate(states):
+            s.set_state(st, member=m)
+    except BaseException:
+        s.close()
+        raise
     return s
 
 

@@ -187,6 +187,13 @@ class Solver:
         except Exception:
             pass
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
     @property
     def handle(self):
         return self._h

@@ -86,10 +86,10 @@ def run(cfg, state, precision: int = FP64, max_steps: int = 10 ** 7):
     c = cfg.replace(precision=precision)
     c64 = cfg.replace(precision=FP64)
     s = gpu.Solver(c)
-    s.set_state(state)
-    dev = [torch.empty((cfg.ny, cfg.nx), dtype=torch.float64, device="cuda") for _ in range(6)]
     snaps = []
     try:
+        s.set_state(state)
+        dev = [torch.empty((cfg.ny, cfg.nx), dtype=torch.float64, device="cuda") for _ in range(6)]
         oc = s.diag()["output_count"]
         for _ in range(max_steps):
             s.step(1)

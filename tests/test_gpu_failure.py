@@ -72,3 +72,25 @@ def test_bad_arguments_rejected(G):
         s.stage(4, 1e-3)
     with pytest.raises(G.ChimeraError):
         s.set_variant(99)
+
+
+def test_handles_close_at_the_end_of_a_with_block(G):
+    """Solver and Adjoint free their C handles on leaving a with block, an
+    exception included."""
+    import torch
+
+    from chimera_b200.adjoint import Adjoint
+    cfg, st = P.orszag_tang(32)
+    with G.Solver(cfg) as s:
+        s.set_state(st)
+        s.step(1)
+        assert s.handle
+    assert not s.handle
+    with pytest.raises(RuntimeError):
+        with G.Solver(cfg) as s2:
+            raise RuntimeError("inside the block")
+    assert not s2.handle
+    with Adjoint(cfg) as a:
+        U = [torch.from_numpy(x.copy()).cuda() for x in st]
+        a.forward_step(U, 1e-3)
+    assert not a._h
