@@ -36,6 +36,7 @@
 #include <new>
 
 #include "../../include/chimera_gpu.h"
+#include "abi_check.h"
 #include "dual.cuh"
 #include "mhd_device.cuh"
 
@@ -670,7 +671,7 @@ extern "C" int chimera_adjoint_step(chimera_adjoint* a, const double* const* U_n
                                     const double* const* lambda_next, double* const* lambda_n) {
   if (!a || !U_n || !lambda_next || !lambda_n || !(dt > 0.0)) return CHIMERA_ERR_BAD_ARG;
   for (int q = 0; q < 6; ++q)
-    if (!U_n[q] || !lambda_next[q] || !lambda_n[q]) return CHIMERA_ERR_BAD_ARG;
+    if (!doubles_ok({U_n[q], lambda_next[q], lambda_n[q]})) return CHIMERA_ERR_BAD_ARG;
   // U_{n+1} of the tape forward is not needed: write it into the stage-1 adjoint buffer
   int rc = upload_ptrs(a, U_n, lambda_next, lambda_n, a->lA);
   if (rc) return rc;
@@ -688,7 +689,7 @@ extern "C" int chimera_adjoint_forward_step(chimera_adjoint* a, const double* co
                                             double* const* U_next) {
   if (!a || !U_n || !U_next || !(dt > 0.0)) return CHIMERA_ERR_BAD_ARG;
   for (int q = 0; q < 6; ++q)
-    if (!U_n[q] || !U_next[q]) return CHIMERA_ERR_BAD_ARG;
+    if (!doubles_ok({U_n[q], U_next[q]})) return CHIMERA_ERR_BAD_ARG;
   int rc = upload_ptrs(a, U_n, nullptr, nullptr, U_next);
   if (rc) return rc;
   switch (a->g.riemann) {

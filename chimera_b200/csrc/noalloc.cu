@@ -19,6 +19,7 @@
 #include <mutex>
 
 #include "../../include/chimera_gpu.h"
+#include "abi_check.h"
 #include "stage_kernel.cuh"
 
 using namespace chimera;
@@ -89,7 +90,7 @@ int scratch_for_current_device(unsigned char** out, int* device) {
 extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, double* Momx,
                                         double* Momy, double* Energy, double* b_x, double* b_y,
                                         double* t, int* output_count, double* dt_next, void* stream) {
-  if (!cfg || !Mass || !Momx || !Momy || !Energy || !b_x || !b_y || !t || !output_count)
+  if (!cfg || !doubles_ok({Mass, Momx, Momy, Energy, b_x, b_y}) || !t || !output_count)
     return CHIMERA_ERR_BAD_ARG;
   if (cfg->nx < 4 || cfg->ny < 4 || !(cfg->dx > 0.0) || !(cfg->dy > 0.0) || !(cfg->gamma > 1.0) ||
       !(cfg->courant > 0.0) || !(cfg->t_out > 0.0) || *output_count < 1)

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/chimera_gpu.h"
+#include "abi_check.h"
 #include "mhd_device.cuh"
 
 using namespace chimera;
@@ -290,7 +291,7 @@ extern "C" {
 int chimera_op_average_face_to_cell_B(const chimera_cfg* cfg, const double* b_x, const double* b_y, double* Bx,
                                       double* By, void* stream) {
   OP_BEGIN(cfg);
-  if (!b_x || !b_y || !Bx || !By) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({b_x, b_y, Bx, By})) return CHIMERA_ERR_BAD_ARG;
   k_avg_B<<<nblocks(n), NB, 0, s>>>(g, b_x, b_y, Bx, By);
   return finish(s);
 }
@@ -299,7 +300,7 @@ int chimera_op_get_primitive(const chimera_cfg* cfg, const double* Mass, const d
                              const double* Energy, const double* Bx, const double* By, double* rho, double* vx,
                              double* vy, double* P, void* stream) {
   OP_BEGIN(cfg);
-  if (!Mass || !Momx || !Momy || !Energy || !Bx || !By || !rho || !vx || !vy || !P) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({Mass, Momx, Momy, Energy, Bx, By, rho, vx, vy, P})) return CHIMERA_ERR_BAD_ARG;
   k_get_primitive<<<nblocks(n), NB, 0, s>>>(g, Mass, Momx, Momy, Energy, Bx, By, rho, vx, vy, P);
   return finish(s);
 }
@@ -308,7 +309,7 @@ int chimera_op_get_conserved(const chimera_cfg* cfg, const double* rho, const do
                              const double* P, const double* Bx, const double* By, double* Mass, double* Momx,
                              double* Momy, double* Energy, void* stream) {
   OP_BEGIN(cfg);
-  if (!rho || !vx || !vy || !P || !Bx || !By || !Mass || !Momx || !Momy || !Energy) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({rho, vx, vy, P, Bx, By, Mass, Momx, Momy, Energy})) return CHIMERA_ERR_BAD_ARG;
   k_get_conserved<<<nblocks(n), NB, 0, s>>>(g, rho, vx, vy, P, Bx, By, Mass, Momx, Momy, Energy);
   return finish(s);
 }
@@ -316,14 +317,14 @@ int chimera_op_get_conserved(const chimera_cfg* cfg, const double* rho, const do
 int chimera_op_apply_conserved_floors(const chimera_cfg* cfg, double* Mass, double* Momx, double* Momy,
                                       double* Energy, const double* Bx, const double* By, void* stream) {
   OP_BEGIN(cfg);
-  if (!Mass || !Momx || !Momy || !Energy || !Bx || !By) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({Mass, Momx, Momy, Energy, Bx, By})) return CHIMERA_ERR_BAD_ARG;
   k_floors<<<nblocks(n), NB, 0, s>>>(g, Mass, Momx, Momy, Energy, Bx, By);
   return finish(s);
 }
 
 int chimera_op_fill_ghost_cells(const chimera_cfg* cfg, const double* f, double* f_pad, void* stream) {
   OP_BEGIN(cfg);
-  if (!f || !f_pad) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({f, f_pad})) return CHIMERA_ERR_BAD_ARG;
   k_fill_ghost<<<nblocks((long long)(g.nx + 2) * (g.ny + 2)), NB, 0, s>>>(g, f, f_pad);
   return finish(s);
 }
@@ -331,7 +332,7 @@ int chimera_op_fill_ghost_cells(const chimera_cfg* cfg, const double* f, double*
 int chimera_op_compute_gradients(const chimera_cfg* cfg, const double* f_pad, double* f_dx, double* f_dy,
                                  void* stream) {
   OP_BEGIN(cfg);
-  if (!f_pad || !f_dx || !f_dy) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({f_pad, f_dx, f_dy})) return CHIMERA_ERR_BAD_ARG;
   k_slopes<<<nblocks(n), NB, 0, s>>>(g, f_pad, f_dx, f_dy, 0);
   return finish(s);
 }
@@ -339,7 +340,7 @@ int chimera_op_compute_gradients(const chimera_cfg* cfg, const double* f_pad, do
 int chimera_op_apply_slope_limiter(const chimera_cfg* cfg, const double* f_pad, double* f_dx, double* f_dy,
                                    void* stream) {
   OP_BEGIN(cfg);
-  if (!f_pad || !f_dx || !f_dy) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({f_pad, f_dx, f_dy})) return CHIMERA_ERR_BAD_ARG;
   k_slopes<<<nblocks(n), NB, 0, s>>>(g, f_pad, f_dx, f_dy, 1);
   return finish(s);
 }
@@ -348,7 +349,7 @@ int chimera_op_reconstruction(const chimera_cfg* cfg, const double* f, const dou
                               double* f_XL, double* f_XR, double* f_YL, double* f_YR, int rho_or_p,
                               void* stream) {
   OP_BEGIN(cfg);
-  if (!f || !f_dx || !f_dy || !f_XL || !f_XR || !f_YL || !f_YR) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({f, f_dx, f_dy, f_XL, f_XR, f_YL, f_YR})) return CHIMERA_ERR_BAD_ARG;
   k_reconstruction<<<nblocks(n), NB, 0, s>>>(g, f, f_dx, f_dy, f_XL, f_XR, f_YL, f_YR, rho_or_p ? 1 : 0,
                                              cfg->mood ? 1 : 0);
   return finish(s);
@@ -357,10 +358,10 @@ int chimera_op_reconstruction(const chimera_cfg* cfg, const double* f, const dou
 int chimera_op_thermal_pressure_check(const chimera_cfg* cfg, double* const* faces24, const double* const* cell6,
                                       void* stream) {
   OP_BEGIN(cfg);
-  if (!faces24 || !cell6) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({faces24, cell6})) return CHIMERA_ERR_BAD_ARG;
   FacePtrs p;
-  for (int k = 0; k < 24; ++k) { if (!faces24[k]) return CHIMERA_ERR_BAD_ARG; p.f[k] = faces24[k]; }
-  for (int k = 0; k < 6; ++k) { if (!cell6[k]) return CHIMERA_ERR_BAD_ARG; p.cell[k] = cell6[k]; }
+  for (int k = 0; k < 24; ++k) { if (!double_ok(faces24[k])) return CHIMERA_ERR_BAD_ARG; p.f[k] = faces24[k]; }
+  for (int k = 0; k < 6; ++k) { if (!double_ok(cell6[k])) return CHIMERA_ERR_BAD_ARG; p.cell[k] = cell6[k]; }
   k_thermal<<<nblocks(n), NB, 0, s>>>(g, p);
   return finish(s);
 }
@@ -368,10 +369,10 @@ int chimera_op_thermal_pressure_check(const chimera_cfg* cfg, double* const* fac
 int chimera_op_compute_fluxes(const chimera_cfg* cfg, const double* const* in12, double* const* out5,
                               void* stream) {
   OP_BEGIN(cfg);
-  if (!in12 || !out5) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({in12, out5})) return CHIMERA_ERR_BAD_ARG;
   FluxPtrs p;
-  for (int k = 0; k < 12; ++k) { if (!in12[k]) return CHIMERA_ERR_BAD_ARG; p.in[k] = in12[k]; }
-  for (int k = 0; k < 5; ++k) { if (!out5[k]) return CHIMERA_ERR_BAD_ARG; p.out[k] = out5[k]; }
+  for (int k = 0; k < 12; ++k) { if (!double_ok(in12[k])) return CHIMERA_ERR_BAD_ARG; p.in[k] = in12[k]; }
+  for (int k = 0; k < 5; ++k) { if (!double_ok(out5[k])) return CHIMERA_ERR_BAD_ARG; p.out[k] = out5[k]; }
   if (g.riemann == CHIMERA_RIEMANN_RUSANOV) k_fluxes<RIEMANN_RUSANOV><<<nblocks(n), NB, 0, s>>>(g, p);
   else if (g.riemann == CHIMERA_RIEMANN_HLLE) k_fluxes<RIEMANN_HLLE><<<nblocks(n), NB, 0, s>>>(g, p);
   else k_fluxes<RIEMANN_HLLD><<<nblocks(n), NB, 0, s>>>(g, p);
@@ -381,7 +382,7 @@ int chimera_op_compute_fluxes(const chimera_cfg* cfg, const double* const* in12,
 int chimera_op_update_conserved(const chimera_cfg* cfg, double* F, const double* flux_X, const double* flux_Y,
                                 double dt, void* stream) {
   OP_BEGIN(cfg);
-  if (!F || !flux_X || !flux_Y) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({F, flux_X, flux_Y})) return CHIMERA_ERR_BAD_ARG;
   k_update_x<<<nblocks(n), NB, 0, s>>>(g, F, flux_X, dt * g.dy);
   k_update_y<<<nblocks(n), NB, 0, s>>>(g, F, flux_Y, dt * g.dx);
   return finish(s);
@@ -391,7 +392,7 @@ int chimera_op_update_conserved(const chimera_cfg* cfg, double* F, const double*
 int chimera_op_constrained_transport(const chimera_cfg* cfg, double* b_x, double* b_y, const double* flux_By_X,
                                      const double* flux_Bx_Y, double dt, double* scratch, void* stream) {
   OP_BEGIN(cfg);
-  if (!b_x || !b_y || !flux_By_X || !flux_Bx_Y || !scratch) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({b_x, b_y, flux_By_X, flux_Bx_Y, scratch})) return CHIMERA_ERR_BAD_ARG;
   k_neg_ez<<<nblocks(n), NB, 0, s>>>(g, flux_By_X, flux_Bx_Y, scratch);
   k_curl_add<<<nblocks(n), NB, 0, s>>>(g, scratch, b_x, b_y, dt, 1);
   return finish(s);
@@ -399,7 +400,7 @@ int chimera_op_constrained_transport(const chimera_cfg* cfg, double* b_x, double
 
 int chimera_op_compute_curl_2d(const chimera_cfg* cfg, const double* Az, double* b_x, double* b_y, void* stream) {
   OP_BEGIN(cfg);
-  if (!Az || !b_x || !b_y) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({Az, b_x, b_y})) return CHIMERA_ERR_BAD_ARG;
   k_curl_add<<<nblocks(n), NB, 0, s>>>(g, Az, b_x, b_y, 1.0, 0);
   return finish(s);
 }
@@ -407,7 +408,7 @@ int chimera_op_compute_curl_2d(const chimera_cfg* cfg, const double* Az, double*
 int chimera_op_compute_divB(const chimera_cfg* cfg, const double* b_x, const double* b_y, double* divB,
                             void* stream) {
   OP_BEGIN(cfg);
-  if (!b_x || !b_y || !divB) return CHIMERA_ERR_BAD_ARG;
+  if (!doubles_ok({b_x, b_y, divB})) return CHIMERA_ERR_BAD_ARG;
   k_divb<<<nblocks(n), NB, 0, s>>>(g, b_x, b_y, divB);
   return finish(s);
 }

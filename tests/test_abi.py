@@ -152,3 +152,26 @@ def test_unit_ops_reject_bad_config(lib, kw, code):
     P = C.c_void_p
     assert lib.chimera_op_average_face_to_cell_B(C.byref(cfg), P(8), P(8), P(8), P(8), None) == code
     assert lib.chimera_op_compute_divB(C.byref(cfg), P(8), P(8), P(8), None) == code
+
+
+def test_misaligned_pointers_refused_before_any_device_call(lib):
+    """Entry points whose kernels use the caller's arrays directly refuse a
+    pointer that is not aligned for double (it would fault a launch).  With
+    every pointer aligned the same calls get past the check and, on a machine
+    without a GPU, stop at their first CUDA call instead."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the refusal without a device")
+    cfg = _cfg()
+    P = C.c_void_p
+    good, odd = P(64), P(64 + 4)
+    avg = lib.chimera_op_average_face_to_cell_B
+    assert avg(C.byref(cfg), good, good, good, odd, None) == -1
+    assert avg(C.byref(cfg), good, good, good, good, None) not in (0, -1)
+    assert lib.chimera_op_compute_divB(C.byref(cfg), odd, good, good, None) == -1
+    t, oc = C.c_double(0.0), C.c_int(1)
+    step = lib.chimera_rk3_step_noalloc
+    args = [good] * 6
+    assert step(C.byref(cfg), *args, C.byref(t), C.byref(oc), None, None) not in (0, -1)
+    args[2] = odd
+    assert step(C.byref(cfg), *args, C.byref(t), C.byref(oc), None, None) == -1
