@@ -205,3 +205,52 @@ def test_gloo_ranks_equal_the_whole_grid(oracle, kind, world):
         got = np.concatenate([r[1][qf] for r in res], axis=0)
         assert np.array_equal(got, ref.a[qf]), qf
     assert all(r[2] == ref.t for r in res)
+
+
+def _leaving_worker(rank, world, port, leave_rank, steps_before, out):
+    """Rank ``leave_rank`` leaves after ``steps_before`` steps, between steps
+    and with nothing in flight; the others go on stepping."""
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    cfg, st = problems.orszag_tang(48)
+    s = OracleSlab(cfg, rank, world)
+    s.set_global_state(st)
+    try:
+        slab_step([s], DistTransport(), steps_before)
+        if rank == leave_rank:
+            out.put((rank, "left"))
+            out.close()
+            out.join_thread()
+            os._exit(3)
+        slab_step([s], DistTransport(), 2)
+        out.put((rank, "finished"))
+    except Exception:   # the failure this test expects on the remaining ranks
+        out.put((rank, "error"))
+        out.close()
+        out.join_thread()
+        os._exit(4)
+
+
+def test_a_rank_that_leaves_ends_the_others_exchange_with_an_error():
+    """Failure detection on the host: when one slab's rank exits between
+    steps, the other rank's next ghost-row exchange (or dt minimum) ends with
+    an error within the process group's timeout instead of waiting for good."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaving_worker, args=(r, world, port, 1, 2, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        res = dict(q.get(timeout=120) for _ in range(world))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert res == {0: "error", 1: "left"}
+    assert procs[0].exitcode == 4 and procs[1].exitcode == 3
