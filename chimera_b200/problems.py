@@ -187,17 +187,27 @@ def _rbf_smooth(noise, length, d):
     return np.real(np.fft.ifft2(np.fft.fft2(noise) * np.exp(-0.5 * length * length * k2)))
 
 
-def grf_member(n, seed, length=0.1, cf_cap=3.0):
+def grf_member(n, seed, length=0.1, cf_cap=3.0, mach=None, beta=None):
     """One GRF ensemble member on the periodic unit square: stream function psi
     and vector potential A_z are white Gaussian noise smoothed by a Gaussian
     RBF of length ``length``; v = curl psi scaled to rms V0 ~ U[0.5, 2];
     B = curl A_z (face centred) scaled to rms B0 ~ U[0.2, 1]; rho = p = 1;
     gamma ~ U[1.4, 5/3]; velocities rescaled so max(c_f + |v|) <= cf_cap (the
-    cap step of src/mhd_init.f90:815-831).  Philox-seeded."""
+    cap step of src/mhd_init.f90:815-831).  Philox-seeded.
+
+    ``mach`` / ``beta`` override the drawn rms speed / field with a target
+    sonic Mach number and plasma beta, V0 = mach sqrt(gamma) and
+    B0 = sqrt(2 / beta) at rho = p = 1 (the counterpart of the reference's
+    M_s and beta overrides, exercised by tests/stress/test_stress.py:113-234);
+    the draws are still made, so the rest of the member is the seed's."""
     rng = np.random.Generator(np.random.Philox(seed))
     gamma = rng.uniform(1.4, 5.0 / 3.0)
     V0 = rng.uniform(0.5, 2.0)
     B0 = rng.uniform(0.2, 1.0)
+    if mach is not None:
+        V0 = float(mach) * math.sqrt(gamma)
+    if beta is not None:
+        B0 = math.sqrt(2.0 / float(beta))
     dx = 1.0 / n
     psi = _rbf_smooth(rng.standard_normal((n, n)), length, dx)
     Az = _rbf_smooth(rng.standard_normal((n, n)), length, dx)
