@@ -6,12 +6,11 @@ Every snapshot must have finite, positive density and thermal pressure, the
 total mass must stay put, and the realised Mach number and beta must be in
 the ranges the reference checks.  The GPU path is bit-identical to the oracle
 in FP64 (tests/test_gpu_parity.py), so these hold for it too."""
-import math
-
 import numpy as np
 import pytest
 
 from chimera_b200 import problems as P
+from chimera_b200 import run
 from tests.snapshots import mass_drift, oracle_snapshots
 
 N, SEED = 64, 42                           # tests/stress/test_stress.py GRF_N, GRF_SEED
@@ -23,16 +22,11 @@ def _member(**kw):
     return cfg.replace(t_end=0.05, t_out=0.01), st
 
 
-def _realised(cfg, st, oracle):
-    """Sonic Mach number and plasma beta of the initial state: rms |v| over the
-    mean sound speed, mean thermal pressure over the mean magnetic pressure."""
-    rho, vx, vy, Ptot, Bx, By = oracle.primitives(cfg, st)
-    B2 = Bx * Bx + By * By
-    p = Ptot - 0.5 * B2
-    cs = np.sqrt(cfg.gamma * p / rho)
-    mach = math.sqrt(float(np.mean(vx * vx + vy * vy))) / float(np.mean(cs))
-    beta = float(np.mean(p)) / float(np.mean(0.5 * B2))
-    return mach, beta
+def _realised(cfg, st):
+    """Sonic Mach number and plasma beta of the initial state, as the
+    reference stores them (run.initial_parameters)."""
+    p = run.initial_parameters(cfg, st, 5)
+    return p["M_s"], p["beta"]
 
 
 def _check_run(oracle, cfg, st):
@@ -50,7 +44,7 @@ def _check_run(oracle, cfg, st):
 @pytest.mark.parametrize("seed", [SEED, SEED + 1])
 def test_grf_completes_positive_and_plausible(oracle, seed):
     cfg, st = _member(seed=seed)
-    mach, beta = _realised(cfg, st, oracle)
+    mach, beta = _realised(cfg, st)
     assert cfg.gamma > 1.0
     assert M_S_BOUNDS[0] < mach < M_S_BOUNDS[1]
     assert BETA_BOUNDS[0] < beta < BETA_BOUNDS[1]
@@ -63,7 +57,7 @@ def test_high_mach_stable(oracle):
     cfg, st = _member(mach=5.0)
     _, uncapped = P.grf_member(N, SEED, mach=5.0, cf_cap=1e30)
     assert not np.array_equal(st[1], uncapped[1])        # the cap rescaled the momenta
-    mach, _ = _realised(cfg, st, oracle)
+    mach, _ = _realised(cfg, st)
     assert M_S_BOUNDS[0] < mach < 5.0
     _check_run(oracle, cfg, st)
 
@@ -73,6 +67,6 @@ def test_low_beta_stable(oracle):
     energy, the regime of the proportional pressure floor; the realised beta
     is magnetically dominated (< 0.5)."""
     cfg, st = _member(beta=0.1)
-    _, beta = _realised(cfg, st, oracle)
+    _, beta = _realised(cfg, st)
     assert beta < 0.5
     _check_run(oracle, cfg, st)
