@@ -284,7 +284,8 @@ __global__ void k_divb(OpGeom g, const double* bx, const double* by, double* div
   int rc_ = make_geom((cfg), &g);      \
   if (rc_) return rc_;                 \
   cudaStream_t s = (cudaStream_t)stream; \
-  const long long n = (long long)g.nx * g.ny;
+  const long long n = (long long)g.nx * g.ny; \
+  (void)n;
 
 extern "C" {
 
