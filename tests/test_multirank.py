@@ -1,10 +1,9 @@
-"""The multi-rank ensemble path on CPU: member sharding and a world-size-2
-gloo run whose ranks each advance their shard (with the CPU oracle) and
-reduce only diagnostics."""
+"""The multi-rank ensemble path on CPU: member sharding, and gloo runs of 2
+and 3 ranks whose ranks each advance their shard (with the CPU oracle) and
+gather only diagnostics (chimera_b200.shard.gather_diagnostics)."""
 import os
 import socket
 
-import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -37,45 +36,75 @@ def _free_port():
     return p
 
 
+class OracleBatch:
+    """Members advanced by the CPU oracle, answering ``diag(member=k)`` with
+    the fields a sharded ensemble gathers (t, steps, mass and energy totals;
+    the others zero), in the role of ``gpu.Solver``."""
+
+    def __init__(self, oracle, sizes, members):
+        from chimera_b200 import problems
+        self.oracle = oracle
+        self.members = []
+        for m in members:
+            cfg, st = problems.grf_member(sizes[m], 500 + m)
+            self.members.append((cfg, oracle.State(st), [0]))
+
+    def step(self, n):
+        for cfg, s, count in self.members:
+            count[0] += len(self.oracle.run(cfg, s, n))
+
+    def diag(self, member=0):
+        from chimera_b200.shard import DIAG_FIELDS
+        _, s, count = self.members[member]
+        d = dict.fromkeys(DIAG_FIELDS, 0.0)
+        d.update(t=s.t, steps=count[0], mass=float(s.a[0].sum()), energy=float(s.a[3].sum()))
+        return d
+
+
 def _worker(rank, world, port, sizes, nsteps, out):
-    import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    from chimera_b200 import problems
+    from chimera_b200.shard import gather_diagnostics
     from oracle import oracle
     mine = shard_members([n * n for n in sizes], world, rank)
-    mass = torch.zeros(len(sizes), dtype=torch.float64)
-    for m in mine:
-        cfg, st = problems.grf_member(sizes[m], 500 + m)
-        s = oracle.State(st)
-        oracle.run(cfg, s, nsteps)
-        mass[m] = s.a[0].sum()
-    dist.all_reduce(mass)          # diagnostics only
-    if rank == 0:
-        out.put(mass.numpy().tolist())
+    batch = OracleBatch(oracle, sizes, mine)      # members are independent: no exchange
+    batch.step(nsteps)
+    out.put((rank, gather_diagnostics(batch, mine, len(sizes))))   # diagnostics only
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_match_one_process(oracle):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_gather_every_members_diagnostics(oracle, world):
+    """Each rank advances its shard; after the one all-reduce every rank holds
+    every member's diagnostics, equal to a single process's."""
     sizes = [16, 24, 16, 32, 20]
     nsteps = 3
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, sizes, nsteps, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, sizes, nsteps, q)) for r in range(world)]
     for p in procs:
         p.start()
-    res = q.get(timeout=120)
+    res = dict(q.get(timeout=120) for _ in range(world))
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    from chimera_b200 import problems
-    ref = []
-    for m, n in enumerate(sizes):
-        cfg, st = problems.grf_member(n, 500 + m)
-        s = oracle.State(st)
-        oracle.run(cfg, s, nsteps)
-        ref.append(s.a[0].sum())
-    assert np.array_equal(np.array(res), np.array(ref))
+    one = OracleBatch(oracle, sizes, range(len(sizes)))
+    one.step(nsteps)
+    ref = [one.diag(member=m) for m in range(len(sizes))]
+    for r in range(world):
+        assert len(res[r]) == len(sizes)
+        for m in range(len(sizes)):
+            for f in ("t", "steps", "mass", "energy", "status"):
+                assert res[r][m][f] == ref[m][f], (r, m, f)
+            assert res[r][m]["steps"] == nsteps
+
+
+def test_gather_without_a_process_group_is_local():
+    from chimera_b200.shard import gather_member_rows
+    t = gather_member_rows({1: [1.0, 2.0], 3: [3.0, 4.0]}, 4, 2)
+    assert t.tolist() == [[0.0, 0.0], [1.0, 2.0], [0.0, 0.0], [3.0, 4.0]]
+    with pytest.raises(ValueError):
+        gather_member_rows({4: [0.0, 0.0]}, 4, 2)
