@@ -254,6 +254,9 @@ def cpu_reference_rate(n, steps, max_seconds=30.0, omp_mode=2):
     from oracle import oracle
     oracle.build()
     oracle.set_omp_mode(omp_mode)
+    # every core this process may run on, also under torchrun (which sets
+    # OMP_NUM_THREADS=1 for its ranks)
+    oracle.set_threads(len(os.sched_getaffinity(0)))
     cfg, st = problems.rotor(n)
     cfg = cfg.replace(t_end=1e30)
     s = oracle.State(st)
@@ -711,12 +714,14 @@ def run_adjoint_leg(args):
 
 def main():
     args = parse()
+    if args.impl == "reference":
+        # the CPU reference arm: rank 0 alone times it, the other ranks exit at
+        # once; no rank takes a collective step, so no process group is made
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
     world, rank, local = dist_setup(args)
     try:
-        if args.impl == "reference":
-            run_reference(args, world, rank)
-        else:
-            run_chimera(args, world, rank, local)
+        run_chimera(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

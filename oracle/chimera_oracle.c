@@ -77,6 +77,14 @@ int orc_max_threads(void) {
     return 1;
 #endif
 }
+/* Thread count of the OpenMP loops (n >= 1), whatever OMP_NUM_THREADS says. */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n >= 1) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
 #define OMP_REF (g_omp_mode >= 1)
 #define OMP_ALL (g_omp_mode >= 2)
 

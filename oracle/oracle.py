@@ -105,6 +105,11 @@ def max_threads() -> int:
     return int(lib().orc_max_threads())
 
 
+def set_threads(n: int) -> None:
+    """Thread count of the OpenMP loops, overriding OMP_NUM_THREADS."""
+    lib().orc_set_threads(int(n))
+
+
 # --- routine-level wrappers (names follow the reference) ----------------------
 
 def average_face_to_cell_B(cfg, b_x, b_y):
