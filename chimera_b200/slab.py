@@ -179,6 +179,13 @@ class SlabSolver:
     def close(self):
         self.solver.close()
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
 
 class LocalTransport:
     """All slabs in this process: ghost rows and dt by device copies."""
