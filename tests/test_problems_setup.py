@@ -1,0 +1,103 @@
+"""The host set-ups of chimera_b200.problems against the reference's set-up
+routines: each initial state is rebuilt here from the reference's formulas and
+constants (src/mhd_config.f90:54-56, cell centres (i - 1/2) dx of
+src/main.f90:36-40), through the oracle's restatements of the reference
+routines the set-ups call (compute_curl_2d, average_face_to_cell_B, and
+get_conserved as src/main.f90:49 applies it), and must equal the package's
+state bit for bit.  The rotor is rebuilt by the reference's per-cell loop."""
+import math
+
+import numpy as np
+
+from chimera_b200 import problems as P
+from oracle.oracle import Config
+
+PI = 3.1415926535897932
+TWO_PI = 6.2831853071795865
+FOUR_PI = 12.566370614359173
+
+
+def _grid(n):
+    dx = 1.0 / n
+    xlin = (np.arange(1, n + 1, dtype=np.float64) - 0.5) * dx
+    X = np.ascontiguousarray(np.broadcast_to(xlin[None, :], (n, n)))   # X(ix, iy) = xlin(ix)
+    Y = np.ascontiguousarray(np.broadcast_to(xlin[:, None], (n, n)))   # Y(ix, iy) = xlin(iy)
+    return dx, xlin, X, Y
+
+
+def _oracle_cfg(cfg):
+    return Config(nx=cfg.nx, ny=cfg.ny, dx=cfg.dx, dy=cfg.dy, gamma=cfg.gamma, bc=cfg.bc)
+
+
+def _conserved(oracle, cfg, rho, vx, vy, p_thermal, b_x, b_y, Bx=None, By=None):
+    c = _oracle_cfg(cfg)
+    if Bx is None:
+        Bx, By = oracle.average_face_to_cell_B(c, b_x, b_y)
+    P_total = p_thermal + 0.5 * (Bx * Bx + By * By)
+    M, Mx, My, E = oracle.get_conserved(c, *[np.ascontiguousarray(a) for a in (rho, vx, vy, P_total, Bx, By)])
+    return [M, Mx, My, E, b_x, b_y]
+
+
+def _assert_same(got, want):
+    for q, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a, b), q
+
+
+def test_orszag_tang_is_setup_OT_vortex(oracle):
+    """src/mhd_init.f90:296-311."""
+    n = 48
+    cfg, st = P.orszag_tang(n)
+    dx, _, X, Y = _grid(n)
+    assert cfg.bc == (1, 1, 1, 1) and cfg.dx == dx
+    rho = np.full((n, n), 25.0 / (36.0 * PI))
+    p = np.full((n, n), 5.0 / (12.0 * PI))
+    vx = -np.sin(TWO_PI * Y)
+    vy = np.sin(TWO_PI * X)
+    Az = np.cos(FOUR_PI * X) / (FOUR_PI * math.sqrt(FOUR_PI)) + np.cos(TWO_PI * Y) / (TWO_PI * math.sqrt(FOUR_PI))
+    b_x, b_y = oracle.compute_curl_2d(_oracle_cfg(cfg), np.ascontiguousarray(Az))
+    _assert_same(st, _conserved(oracle, cfg, rho, vx, vy, p, b_x, b_y))
+
+
+def test_field_loop_is_setup_FL_advec(oracle):
+    """src/mhd_init.f90:360-391 (unit square, v = (-2, -1))."""
+    n = 40
+    cfg, st = P.field_loop(n, n, 1.0, 1.0, v=(-2.0, -1.0))
+    dx, _, X, Y = _grid(n)
+    r0, A0, x0, y0 = 0.3, 1.0e-3, 0.5, 0.5
+    r = np.sqrt((X - x0) ** 2 + (Y - y0) ** 2)
+    Az = np.where(r < r0, A0 * (r0 - r), 0.0)
+    b_x, b_y = oracle.compute_curl_2d(_oracle_cfg(cfg), np.ascontiguousarray(Az))
+    ones = np.ones((n, n))
+    _assert_same(st, _conserved(oracle, cfg, ones, -2.0 * ones, -1.0 * ones, ones, b_x, b_y))
+
+
+def test_rotor_is_setup_rotor(oracle):
+    """src/mhd_init.f90:399-450, by its per-cell loop."""
+    n = 40
+    cfg, st = P.rotor(n)
+    dx, xlin, _, _ = _grid(n)
+    assert cfg.bc == (3, 3, 3, 3) and cfg.gamma == 1.4
+    x0 = y0 = 0.5
+    r0, r1, u0 = 0.1, 0.115, 2.0
+    rho = np.ones((n, n))
+    vx = np.zeros((n, n))
+    vy = np.zeros((n, n))
+    for iy in range(n):
+        for ix in range(n):
+            rx = float(xlin[ix]) - x0
+            ry = float(xlin[iy]) - y0
+            r = math.sqrt(rx * rx + ry * ry)
+            if r <= r0:
+                rho[iy, ix] = 10.0
+                vx[iy, ix] = -(u0 * (ry / r0))
+                vy[iy, ix] = u0 * (rx / r0)
+            elif r < r1:
+                f = (r1 - r) / (r1 - r0)
+                rho[iy, ix] = 1.0 + 9.0 * f
+                if r > 0.0:
+                    vx[iy, ix] = -(f * u0 * (ry / r))
+                    vy[iy, ix] = f * u0 * (rx / r)
+    Bx = np.full((n, n), 5.0 / math.sqrt(4.0 * PI))
+    By = np.zeros((n, n))
+    b_x, b_y = Bx.copy(), By.copy()             # face B = the uniform cell B
+    _assert_same(st, _conserved(oracle, cfg, rho, vx, vy, np.ones((n, n)), b_x, b_y, Bx, By))
