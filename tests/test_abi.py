@@ -175,3 +175,17 @@ def test_misaligned_pointers_refused_before_any_device_call(lib):
     assert step(C.byref(cfg), *args, C.byref(t), C.byref(oc), None, None) not in (0, -1)
     args[2] = odd
     assert step(C.byref(cfg), *args, C.byref(t), C.byref(oc), None, None) == -1
+
+
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c++", "-std=c++11")])
+def test_header_is_plain_c_and_cpp(lang, std, tmp_path):
+    """include/chimera_gpu.h stands alone as C99 and C++11 (no CUDA headers), so
+    C, C++ and Fortran-side build systems can use it as it is."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-x", lang, HEADER],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
