@@ -189,3 +189,73 @@ def test_header_is_plain_c_and_cpp(lang, std, tmp_path):
     r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-x", lang, HEADER],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+_LAYOUT_C = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "chimera_gpu.h"
+#define F(S, f) printf(#S " " #f " %zu %zu\n", offsetof(S, f), sizeof(((S*)0)->f));
+int main(void) {
+  printf("chimera_cfg SIZE %zu 0\n", sizeof(chimera_cfg));
+  printf("chimera_diag_out SIZE %zu 0\n", sizeof(chimera_diag_out));
+  F(chimera_cfg, nx) F(chimera_cfg, ny) F(chimera_cfg, dx) F(chimera_cfg, dy) F(chimera_cfg, gamma)
+  F(chimera_cfg, courant) F(chimera_cfg, t_out) F(chimera_cfg, t_end) F(chimera_cfg, bc_xlo)
+  F(chimera_cfg, bc_xhi) F(chimera_cfg, bc_ylo) F(chimera_cfg, bc_yhi) F(chimera_cfg, riemann)
+  F(chimera_cfg, limiter) F(chimera_cfg, use_slope_limiting) F(chimera_cfg, mood) F(chimera_cfg, precision)
+  F(chimera_diag_out, t) F(chimera_diag_out, dt) F(chimera_diag_out, output_count)
+  F(chimera_diag_out, active) F(chimera_diag_out, steps) F(chimera_diag_out, divb_max)
+  F(chimera_diag_out, divb_mean) F(chimera_diag_out, bmax) F(chimera_diag_out, divb_rel)
+  F(chimera_diag_out, mass) F(chimera_diag_out, energy) F(chimera_diag_out, cfl_speed)
+  F(chimera_diag_out, mood_resets) F(chimera_diag_out, floor_hits) F(chimera_diag_out, status)
+  return 0;
+}
+"""
+
+
+def _c_layout(tmp_path):
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / "layout.c"
+    src.write_text(_LAYOUT_C)
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    out = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        s, f, off, size = line.split()
+        out.setdefault(s, []).append((f, int(off), int(size)))
+    return out
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The ctypes mirrors of chimera_cfg / chimera_diag_out (chimera_b200.gpu)
+    have the header's field order, offsets, sizes and total size."""
+    from chimera_b200 import gpu
+    lay = _c_layout(tmp_path)
+    for name, cls in (("chimera_cfg", gpu.CCfg), ("chimera_diag_out", gpu.CDiag)):
+        size = [e for e in lay[name] if e[0] == "SIZE"][0][1]
+        fields = [e for e in lay[name] if e[0] != "SIZE"]
+        assert C.sizeof(cls) == size, name
+        assert [f for f, _ in cls._fields_] == [f for f, _, _ in fields], name
+        for f, off, sz in fields:
+            assert getattr(cls, f).offset == off and getattr(cls, f).size == sz, (name, f)
+
+
+def test_fortran_types_match_the_header(tmp_path):
+    """The bind(C) derived types of the Fortran module list the header's fields
+    in the same order with interoperable kinds of the same sizes."""
+    lay = _c_layout(tmp_path)
+    text = open(FORTRAN).read()
+    kinds = {"c_int": 4, "c_double": 8, "c_long_long": 8}
+    for name in ("chimera_cfg", "chimera_diag_out"):
+        body = re.search(rf"type, bind\(C\) :: {name}\n(.*?)end type {name}", text, flags=re.S).group(1)
+        got = []
+        for line in body.splitlines():
+            m = re.match(r"\s*(?:integer|real)\((c_\w+)\)\s*::\s*(.+)", line)
+            if m:
+                got += [(f.strip(), kinds[m.group(1)]) for f in m.group(2).split(",")]
+        want = [(f, sz) for f, _, sz in lay[name] if f != "SIZE"]
+        assert got == want, name
