@@ -259,3 +259,47 @@ def test_fortran_types_match_the_header(tmp_path):
                 got += [(f.strip(), kinds[m.group(1)]) for f in m.group(2).split(",")]
         want = [(f, sz) for f, _, sz in lay[name] if f != "SIZE"]
         assert got == want, name
+
+
+def _c_conventions(path):
+    """name -> (return kind, [per-parameter 'ptr' | 'val']) of every prototype."""
+    text = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
+    text = re.sub(r"#.*", "", text)
+    out = {}
+    for ret, name, params in re.findall(r"([A-Za-z_][\w\s\*]*?)\b(chimera_\w+)\s*\(([^;{]*?)\)\s*;", text,
+                                        flags=re.S):
+        ret = ret.split(";")[-1].split("}")[-1].strip()
+        rk = "sub" if ret == "void" else ("ptr" if "*" in ret else "int")
+        p = params.strip()
+        kinds = [] if p in ("", "void") else ["ptr" if "*" in a else "val" for a in p.split(",")]
+        out[name] = (rk, kinds)
+    return out
+
+
+def _fortran_conventions(path):
+    """bind(C) name -> (return kind, [per-argument 'ptr' | 'val']): an argument
+    with the value attribute is passed by value unless it is a type(c_ptr)
+    (a pointer passed by value); any other argument is passed by reference."""
+    text = open(path).read().replace("&\n", " ")
+    out = {}
+    pat = re.compile(r"^\s*(integer\(c_int\)\s+function|type\(c_ptr\)\s+function|subroutine)\s+\w+\s*"
+                     r"\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)(.*?)^\s*end\s+(?:function|subroutine)",
+                     flags=re.S | re.M)
+    for head, args, name, body in pat.findall(text):
+        rk = "sub" if head.startswith("subroutine") else ("ptr" if head.startswith("type") else "int")
+        decl = {}
+        for m in re.finditer(r"^\s*(type\(\w+\)|integer\(\w+\)|real\(\w+\))([^:\n]*)::\s*(.+)$", body, flags=re.M):
+            typ, attrs, names = m.groups()
+            for nm in re.sub(r"\([^)]*\)", "", names).split(","):
+                decl[nm.strip()] = "val" if ("value" in attrs and typ != "type(c_ptr)") else "ptr"
+        out[name] = (rk, [decl[a.strip()] for a in args.split(",") if a.strip()])
+    return out
+
+
+def test_fortran_module_passes_every_argument_as_the_header_takes_it():
+    """Scalars by value where the C parameter is a scalar, addresses (by
+    reference, or a type(c_ptr) by value) where it is a pointer, and the
+    return kinds (int / pointer / none) of the header."""
+    c, f = _c_conventions(HEADER), _fortran_conventions(FORTRAN)
+    assert set(f) == set(c), sorted(set(c) ^ set(f))
+    assert {k: (c[k], f[k]) for k in c if c[k] != f[k]} == {}
