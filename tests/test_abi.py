@@ -271,15 +271,16 @@ def _c_conventions(path):
         ret = ret.split(";")[-1].split("}")[-1].strip()
         rk = "sub" if ret == "void" else ("ptr" if "*" in ret else "int")
         p = params.strip()
-        kinds = [] if p in ("", "void") else ["ptr" if "*" in a else "val" for a in p.split(",")]
+        kinds = [] if p in ("", "void") else [("val", "ptr", "ptr2")[min(a.count("*"), 2)] for a in p.split(",")]
         out[name] = (rk, kinds)
     return out
 
 
 def _fortran_conventions(path):
-    """bind(C) name -> (return kind, [per-argument 'ptr' | 'val']): an argument
-    with the value attribute is passed by value unless it is a type(c_ptr)
-    (a pointer passed by value); any other argument is passed by reference."""
+    """bind(C) name -> (return kind, [per-argument 'val' | 'ptr' | 'ptr2']):
+    with the value attribute an argument is a scalar, or a pointer if it is a
+    type(c_ptr); without it the argument's address is passed -- a pointer, or
+    a pointer to a pointer for a type(c_ptr) (an array of them included)."""
     text = open(path).read().replace("&\n", " ")
     out = {}
     pat = re.compile(r"^\s*(integer\(c_int\)\s+function|type\(c_ptr\)\s+function|subroutine)\s+\w+\s*"
@@ -291,15 +292,17 @@ def _fortran_conventions(path):
         for m in re.finditer(r"^\s*(type\(\w+\)|integer\(\w+\)|real\(\w+\))([^:\n]*)::\s*(.+)$", body, flags=re.M):
             typ, attrs, names = m.groups()
             for nm in re.sub(r"\([^)]*\)", "", names).split(","):
-                decl[nm.strip()] = "val" if ("value" in attrs and typ != "type(c_ptr)") else "ptr"
+                byval, cptr = "value" in attrs, typ == "type(c_ptr)"
+                decl[nm.strip()] = ("ptr" if cptr else "val") if byval else ("ptr2" if cptr else "ptr")
         out[name] = (rk, [decl[a.strip()] for a in args.split(",") if a.strip()])
     return out
 
 
 def test_fortran_module_passes_every_argument_as_the_header_takes_it():
-    """Scalars by value where the C parameter is a scalar, addresses (by
-    reference, or a type(c_ptr) by value) where it is a pointer, and the
-    return kinds (int / pointer / none) of the header."""
+    """Scalars by value where the C parameter is a scalar; one level of
+    address (a type(c_ptr) by value, or another argument by reference) where it
+    is a pointer; a type(c_ptr) by reference where it is a pointer to a
+    pointer; and the header's return kinds (int / pointer / none)."""
     c, f = _c_conventions(HEADER), _fortran_conventions(FORTRAN)
     assert set(f) == set(c), sorted(set(c) ^ set(f))
     assert {k: (c[k], f[k]) for k in c if c[k] != f[k]} == {}
