@@ -306,3 +306,57 @@ def test_fortran_module_passes_every_argument_as_the_header_takes_it():
     c, f = _c_conventions(HEADER), _fortran_conventions(FORTRAN)
     assert set(f) == set(c), sorted(set(c) ^ set(f))
     assert {k: (c[k], f[k]) for k in c if c[k] != f[k]} == {}
+
+
+def _c_params(path):
+    """name -> (return text, [(level of indirection, base type)]) of every prototype."""
+    text = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
+    text = re.sub(r"#.*", "", text)
+    out = {}
+    for ret, name, params in re.findall(r"([A-Za-z_][\w\s\*]*?)\b(chimera_\w+)\s*\(([^;{]*?)\)\s*;", text,
+                                        flags=re.S):
+        ret = ret.split(";")[-1].split("}")[-1].strip()
+        p = params.strip()
+        plist = []
+        if p not in ("", "void"):
+            for a in p.split(","):
+                words = a.replace("*", " ").replace("const", " ").split()
+                plist.append((a.count("*"), " ".join(words[:-1])))
+        out[name] = (ret, plist)
+    return out
+
+
+def test_ctypes_argtypes_match_the_header(lib):
+    """Every argtypes / restype the Python bindings declare (chimera_b200.gpu,
+    .ops, .adjoint) agrees with the header: int and double scalars as c_int
+    and c_double, pointers as pointers, pointers to pointers as arrays of or
+    pointers to c_void_p (an opaque c_void_p is accepted for either)."""
+    from chimera_b200 import adjoint, ops
+    ops._lib()
+    adjoint._lib()
+    scalars = {"int": C.c_int, "double": C.c_double}
+    checked = 0
+    for name, (ret, params) in _c_params(HEADER).items():
+        fn = getattr(lib, name)
+        if fn.argtypes is None:
+            continue
+        checked += 1
+        assert len(fn.argtypes) == len(params), name
+        for k, (t, (level, base)) in enumerate(zip(fn.argtypes, params)):
+            if level == 0:
+                assert t is scalars[base], (name, k)
+            elif t is C.c_void_p or t is C.c_char_p:
+                continue
+            elif level == 1:
+                assert issubclass(t, C._Pointer) and t._type_ is not C.c_void_p, (name, k)
+            else:
+                ok_array = issubclass(t, C.Array) and t._type_ is C.c_void_p
+                ok_ptr = issubclass(t, C._Pointer) and t._type_ is C.c_void_p
+                assert ok_array or ok_ptr, (name, k)
+        if ret == "void":
+            assert fn.restype is None, name
+        elif "*" in ret:
+            assert fn.restype in (C.c_void_p, C.c_char_p), name
+        else:
+            assert fn.restype is C.c_int, name
+    assert checked >= 40
