@@ -360,3 +360,28 @@ def test_ctypes_argtypes_match_the_header(lib):
         else:
             assert fn.restype is C.c_int, name
     assert checked >= 40
+
+
+def test_constants_agree_across_the_bindings():
+    """The header's switch, location, precision and error constants have the
+    same values in the Python package and the Fortran module."""
+    from chimera_b200 import config, gpu
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    h = {k: int(v) for k, v in re.findall(r"#define\s+(CHIMERA_\w+)\s+(-?\d+)\s*$", text, flags=re.M)}
+    py = {
+        "CHIMERA_RIEMANN_RUSANOV": config.RUSANOV, "CHIMERA_RIEMANN_HLLE": config.HLLE,
+        "CHIMERA_RIEMANN_HLLD": config.HLLD, "CHIMERA_LIMITER_VAN_LEER": config.VAN_LEER,
+        "CHIMERA_LIMITER_MC": config.MC, "CHIMERA_BC_PERIODIC": config.BC_PERIODIC,
+        "CHIMERA_BC_FIXED": config.BC_FIXED, "CHIMERA_BC_OUTFLOW": config.BC_OUTFLOW,
+        "CHIMERA_BC_INFLOW": config.BC_INFLOW, "CHIMERA_FP64": config.FP64,
+        "CHIMERA_FP32_BULK": config.FP32_BULK, "CHIMERA_HOST": gpu.HOST, "CHIMERA_DEVICE": gpu.DEVICE,
+        "CHIMERA_OK": gpu.OK,
+    }
+    py.update({name: code for code, name in gpu.ERR.items()})
+    assert {k: (h.get(k), v) for k, v in py.items() if h.get(k) != v} == {}
+    assert sorted(k for k in h if k.startswith("CHIMERA_ERR_")) == sorted(gpu.ERR.values())
+    f = {}
+    for decl in re.findall(r"parameter\s*::\s*(.+)", open(FORTRAN).read()):
+        for name, val in re.findall(r"(CHIMERA_\w+)\s*=\s*(-?\d+)", decl):
+            f[name] = int(val)
+    assert f and {k: (h.get(k), v) for k, v in f.items() if h.get(k) != v} == {}
