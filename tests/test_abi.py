@@ -37,9 +37,12 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_strerror(lib):
+    from chimera_b200.gpu import ERR
     assert lib.chimera_strerror(0) == b"ok"
     assert b"invalid" in lib.chimera_strerror(-1)
     assert lib.chimera_strerror(12345) == b"unknown error"
+    texts = [lib.chimera_strerror(code) for code in ERR]     # every error code has its own text
+    assert b"unknown error" not in texts and len(set(texts)) == len(ERR)
 
 
 def _cfg(**kw):
