@@ -108,3 +108,50 @@ def test_gather_without_a_process_group_is_local():
     assert t.tolist() == [[0.0, 0.0], [1.0, 2.0], [0.0, 0.0], [3.0, 4.0]]
     with pytest.raises(ValueError):
         gather_member_rows({4: [0.0, 0.0]}, 4, 2)
+
+
+def _leaving_worker(rank, world, port, sizes, out):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    from chimera_b200.shard import gather_diagnostics
+    from oracle import oracle
+    mine = shard_members([n * n for n in sizes], world, rank)
+    batch = OracleBatch(oracle, sizes, mine)
+    batch.step(2)
+    if rank == 1:                    # leaves after its steps, before the gather
+        out.put((rank, "left"))
+        out.close()
+        out.join_thread()
+        os._exit(3)
+    try:
+        gather_diagnostics(batch, mine, len(sizes))
+        out.put((rank, "gathered"))
+    except Exception:   # the failure this test expects
+        out.put((rank, "error"))
+    out.close()
+    out.join_thread()
+    os._exit(4)
+
+
+def test_a_rank_that_leaves_ends_the_gather_with_an_error():
+    """Failure detection on the host: when a rank of a sharded ensemble exits
+    before the diagnostics gather, the other rank's gather ends with an error
+    within the process group's timeout instead of waiting for good."""
+    sizes = [16, 24, 16, 20]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaving_worker, args=(r, 2, port, sizes, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        res = dict(q.get(timeout=120) for _ in range(2))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert res == {0: "error", 1: "left"}
