@@ -4,7 +4,10 @@ constants (src/mhd_config.f90:54-56, cell centres (i - 1/2) dx of
 src/main.f90:36-40), through the oracle's restatements of the reference
 routines the set-ups call (compute_curl_2d, average_face_to_cell_B, and
 get_conserved as src/main.f90:49 applies it), and must equal the package's
-state bit for bit.  The rotor is rebuilt by the reference's per-cell loop."""
+state bit for bit.  The rotor is rebuilt by the reference's per-cell loop.
+The Kelvin-Helmholtz and adjoint field-loop workloads follow their own
+specifications instead (domain, speeds, noise); those are checked against
+their formulas."""
 import math
 
 import numpy as np
@@ -101,3 +104,48 @@ def test_rotor_is_setup_rotor(oracle):
     By = np.zeros((n, n))
     b_x, b_y = Bx.copy(), By.copy()             # face B = the uniform cell B
     _assert_same(st, _conserved(oracle, cfg, rho, vx, vy, np.ones((n, n)), b_x, b_y, Bx, By))
+
+
+def test_kelvin_helmholtz_follows_its_specification(oracle):
+    """The Kelvin-Helmholtz workload (not the reference's top-hat set-up):
+    [0,1] x [-1,1] periodic, gamma 1.4, HLLD; rho = 1, p = 2.5,
+    vx = 0.5 tanh(y'/0.05) with y' mirrored at |y| = 1/2, vy = 0.01 sin(2 pi x)
+    exp(-y^2/0.01) + uniform noise of amplitude 1e-3 (seeded), Bx = 0.1."""
+    n = 64
+    cfg, st = P.kelvin_helmholtz(n)
+    assert (cfg.dx, cfg.dy, cfg.gamma, cfg.riemann, cfg.bc) == (1.0 / n, 2.0 / n, 1.4, 3, (1, 1, 1, 1))
+    rho, vx, vy, Ptot, Bx, By = oracle.primitives(cfg, st)
+    x = (np.arange(1, n + 1) - 0.5) / n
+    y = -1.0 + (np.arange(1, n + 1) - 0.5) * 2.0 / n
+    X, Y = np.meshgrid(x, y)
+    ym = np.where(Y > 0.5, 1.0 - Y, np.where(Y < -0.5, -1.0 - Y, Y))
+    assert np.array_equal(rho, np.ones((n, n)))
+    assert np.max(np.abs(Bx - 0.1)) == 0.0 and np.max(np.abs(By)) == 0.0
+    assert np.max(np.abs((Ptot - 0.5 * (Bx * Bx + By * By)) - 2.5)) < 1e-13
+    assert np.max(np.abs(vx - 0.5 * np.tanh(ym / 0.05))) < 1e-15
+    noise = vy - 0.01 * np.sin(2.0 * np.pi * X) * np.exp(-Y * Y / 0.01)
+    assert np.max(np.abs(noise)) <= 1e-3 * (1 + 1e-12)
+    assert 0.5e-3 < noise.std() < 0.65e-3 and abs(noise.mean()) < 1e-4
+    assert np.array_equal(P.kelvin_helmholtz(n)[1][2], st[2])            # seeded
+    assert not np.array_equal(P.kelvin_helmholtz(n, seed=1)[1][2], st[2])
+
+
+def test_adjoint_field_loop_follows_its_specification(oracle):
+    """The adjoint workload's field loop: [0,2] x [0,1] periodic, v = (2, 1),
+    HLLE + Van Leer, gamma 5/3, rho = p = 1, A_z = 1e-3 (0.3 - r) about
+    (1, 0.5), so |B| = 1e-3 inside the loop away from its centre and rim."""
+    cfg, st = P.field_loop(128, 64)
+    assert (cfg.dx, cfg.dy, cfg.gamma, cfg.riemann, cfg.limiter) == (2.0 / 128, 1.0 / 64, 5.0 / 3.0, 2, 1)
+    rho, vx, vy, Ptot, Bx, By = oracle.primitives(cfg, st)
+    assert np.array_equal(rho, np.ones_like(rho))
+    assert np.max(np.abs(vx - 2.0)) < 1e-14 and np.max(np.abs(vy - 1.0)) < 1e-14
+    x = (np.arange(1, 129) - 0.5) * cfg.dx
+    y = (np.arange(1, 65) - 0.5) * cfg.dy
+    X, Y = np.meshgrid(x, y)
+    r = np.sqrt((X - 1.0) ** 2 + (Y - 0.5) ** 2)
+    B = np.sqrt(Bx * Bx + By * By)
+    ring = (r > 0.06) & (r < 0.24)
+    assert np.max(np.abs(B[ring] - 1e-3)) < 5e-5
+    assert np.max(B[r > 0.33]) == 0.0
+    d = oracle.compute_divB(_oracle_cfg(cfg), st[4], st[5])
+    assert np.max(np.abs(d)) < 1e-15
