@@ -192,8 +192,10 @@ def grf_member(n, seed, length=0.1, cf_cap=3.0, mach=None, beta=None):
     and vector potential A_z are white Gaussian noise smoothed by a Gaussian
     RBF of length ``length``; v = curl psi scaled to rms V0 ~ U[0.5, 2];
     B = curl A_z (face centred) scaled to rms B0 ~ U[0.2, 1]; rho = p = 1;
-    gamma ~ U[1.4, 5/3]; velocities rescaled so max(c_f + |v|) <= cf_cap (the
-    cap step of src/mhd_init.f90:815-831).  Philox-seeded.
+    gamma ~ U[1.4, 5/3]; where max(c_f + |v|) exceeds cf_cap the velocities are
+    scaled by cf_cap / max(c_f + |v|) and B is left alone (the cap step of
+    src/mhd_init.f90:811-829, which can leave the maximum above cf_cap when
+    c_f is large).  Philox-seeded.
 
     ``mach`` / ``beta`` override the drawn rms speed / field with a target
     sonic Mach number and plasma beta, V0 = mach sqrt(gamma) and

@@ -149,3 +149,35 @@ def test_adjoint_field_loop_follows_its_specification(oracle):
     assert np.max(B[r > 0.33]) == 0.0
     d = oracle.compute_divB(_oracle_cfg(cfg), st[4], st[5])
     assert np.max(np.abs(d)) < 1e-15
+
+
+def test_grf_members_follow_their_specification(oracle):
+    """GRF ensemble members: periodic unit square, rho = p = 1, gamma in
+    [1.4, 5/3], face-centred B from a smoothed A_z with rms |B| in [0.2, 1],
+    divergence free; velocity with rms |v| in [0.5, 2] before the cap step,
+    which scales the velocities alone by 3 / max(c_f + |v|) where that maximum
+    exceeds 3 (src/mhd_init.f90:811-829)."""
+    n = 64
+    capped = 0
+    for seed in range(8):
+        cfg, st = P.grf_member(n, 1000 + seed)
+        _, raw = P.grf_member(n, 1000 + seed, cf_cap=1e30)
+        assert 1.4 <= cfg.gamma <= 5.0 / 3.0 and cfg.bc == (1, 1, 1, 1) and cfg.dx == 1.0 / n
+        rho, vx, vy, Ptot, Bx, By = oracle.primitives(cfg, st)
+        _, ux, uy, _, _, _ = oracle.primitives(cfg, raw)
+        B2 = Bx * Bx + By * By
+        assert np.max(np.abs(rho - 1.0)) < 1e-15
+        assert np.max(np.abs((Ptot - 0.5 * B2) - 1.0)) < 1e-12
+        assert 0.2 - 1e-12 <= math.sqrt(float(np.mean(B2))) <= 1.0 + 1e-12
+        assert 0.5 - 1e-12 <= math.sqrt(float(np.mean(ux * ux + uy * uy))) <= 2.0 + 1e-12
+        assert np.array_equal(st[4], raw[4]) and np.array_equal(st[5], raw[5])     # B never rescaled
+        top = float(np.max(np.sqrt(cfg.gamma + B2) + np.sqrt(ux * ux + uy * uy)))
+        if top > 3.0:
+            capped += 1
+            nz = np.abs(ux) > 1e-8
+            assert np.max(np.abs(vx[nz] / ux[nz] - 3.0 / top)) < 1e-12
+        else:
+            assert np.array_equal(st[1], raw[1]) and np.array_equal(st[2], raw[2])
+        d = oracle.compute_divB(_oracle_cfg(cfg), st[4], st[5])
+        assert np.max(np.abs(d)) < 1e-12
+    assert 0 < capped < 8          # both branches of the cap step seen
