@@ -52,8 +52,9 @@ def test_grf_completes_positive_and_plausible(oracle, seed):
 
 
 def test_high_mach_stable(oracle):
-    """Target M_s = 5: the rms speed 5 c_s is clipped by the fast-speed cap of
-    3, so the run starts on the cap's path with steep velocity gradients."""
+    """Target M_s = 5: the cap step scales the velocities down by
+    3 / max(c_f + |v|), so the run starts on the cap's path with steep
+    velocity gradients."""
     cfg, st = _member(mach=5.0)
     _, uncapped = P.grf_member(N, SEED, mach=5.0, cf_cap=1e30)
     assert not np.array_equal(st[1], uncapped[1])        # the cap rescaled the momenta
