@@ -203,6 +203,10 @@ class Solver:
         return lib().chimera_stream(self._h) or 0
 
     def set_state(self, arrays: Sequence, member: int = 0):
+        """Six conserved fields (Mass, Momx, Momy, Energy, b_x, b_y) of member
+        ``member`` in: numpy arrays or CPU tensors are read completely before
+        the call returns (page-locked ones included); CUDA tensors are copied
+        in order on the solver's stream."""
         c = self.cfgs[member]
         p, ld, where, keep = _ptrs(arrays, c.nx, c.ny)
         _check(lib().chimera_batch_set_state(self._h, member, *p, ld, where), "set_state")
