@@ -93,7 +93,7 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   if (!cfg || !doubles_ok({Mass, Momx, Momy, Energy, b_x, b_y}) || !t || !output_count)
     return CHIMERA_ERR_BAD_ARG;
   if (cfg->nx < 4 || cfg->ny < 4 || !(cfg->dx > 0.0) || !(cfg->dy > 0.0) || !(cfg->gamma > 1.0) ||
-      !(cfg->courant > 0.0) || !(cfg->t_out > 0.0) || *output_count < 1)
+      !(cfg->courant > 0.0) || !(cfg->t_out > 0.0) || !(cfg->t_end > 0.0) || *output_count < 1)
     return CHIMERA_ERR_BAD_ARG;
   if (cfg->precision != CHIMERA_FP64) return CHIMERA_ERR_UNSUPPORTED;
   for (int b : {cfg->bc_xlo, cfg->bc_xhi, cfg->bc_ylo, cfg->bc_yhi})
@@ -104,13 +104,33 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   if (cfg->riemann < 1 || cfg->riemann > 3 || cfg->limiter < 1 || cfg->limiter > 2) return CHIMERA_ERR_BAD_ARG;
   const size_t cells = size_t(cfg->nx) * size_t(cfg->ny);
   if (cells > NA_MAX_CELLS) return CHIMERA_ERR_TOO_LARGE;
+  // The run is over (src/main.f90:65, do while (t < tEnd)): no step is taken
+  // and nothing is launched; the state, t and output_count stay as they are.
+  if (!(*t < cfg->t_end)) return CHIMERA_OK;
 
   unsigned char* base = nullptr;
   int dev = -1;
   int rc = scratch_for_current_device(&base, &dev);
   if (rc) return rc;
-  std::lock_guard<std::mutex> call_lock(g_call_mutex[dev]);
   cudaStream_t s = (cudaStream_t)stream;
+  if (s) {   // the scratch is the current device's: the stream must be on it too
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      return CHIMERA_ERR_BAD_ARG;
+    }
+    if (sdev != dev) return CHIMERA_ERR_BAD_ARG;
+  }
+  std::lock_guard<std::mutex> call_lock(g_call_mutex[dev]);
+  // Every return after the first launch drains the stream first, while the
+  // lock is held: no kernel of this call may still use the scratch (or the
+  // caller's arrays) once another call can take it.
+  auto fail = [s]() {
+    cudaGetLastError();
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
+    return CHIMERA_ERR_CUDA;
+  };
 
   Member g;
   memset(&g, 0, sizeof(g));
@@ -177,21 +197,18 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
       stage_kernel<double, 3, 3, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
       break;
   }
-  if (cudaGetLastError() != cudaSuccess) return CHIMERA_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return fail();
   // After stage 3 the new state sits in stage buffer 1; copy it back into the
-  // caller's arrays (dense (nx, ny), x fastest).
+  // caller's arrays (dense (nx, ny), x fastest).  The step is always taken
+  // here (t < t_end was checked above, so the CFL kernel leaves it active).
   for (int q = 0; q < 6; ++q) {
-    if (cudaMemcpyAsync(user[q], g.buf[1][q], cells * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
-      cudaGetLastError();
-      return CHIMERA_ERR_CUDA;
-    }
+    if (cudaMemcpyAsync(user[q], g.buf[1][q], cells * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return fail();
   }
   Control c;
   if (cudaMemcpyAsync(&c, d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
-    cudaGetLastError();
-    return CHIMERA_ERR_CUDA;
-  }
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return fail();
   if (dt_next) *dt_next = c.dt;
   *t = c.t;
   *output_count = c.output_count;

@@ -261,15 +261,24 @@ void chimera_adjoint_destroy(chimera_adjoint* a);
  * library holds until the process exits.
  *   - Mass..b_y: device pointers to dense (nx, ny) arrays, x fastest, updated
  *     in place; cfg->precision must be CHIMERA_FP64.
- *   - nx*ny above CHIMERA_NOALLOC_MAX_CELLS returns CHIMERA_ERR_TOO_LARGE.
+ *   - nx*ny above CHIMERA_NOALLOC_MAX_CELLS returns CHIMERA_ERR_TOO_LARGE;
+ *     cfg->t_end must be > 0 (CHIMERA_ERR_BAD_ARG otherwise).
  *   - *t and *output_count are read and advanced; *dt_next (optional) receives
- *     the dt the next step will take.  The call synchronises the stream.
+ *     the dt the next step will take.  The call synchronises the stream, on
+ *     its error paths too.
+ *   - With *t >= cfg->t_end the run is over: the call launches nothing and
+ *     returns CHIMERA_OK with the arrays, *t, *output_count and *dt_next
+ *     untouched (as chimera_step leaves an inactive state).
+ *   - stream (null = the current device's legacy stream) must belong to the
+ *     current device, whose scratch the call uses; CHIMERA_ERR_BAD_ARG if not.
  *   - The first call on a device looks up the scratch's device address; make
  *     that first call before any stream capture.
- *   - Every call shares the one scratch array of its device.  Calls from
- *     several host threads of one process are serialised per device inside
- *     the library; calls from other processes use their own copy.  A call
- *     made during a stream capture is not supported (it synchronises). */
+ *   - Every call shares the one scratch array of its device, which keeps the
+ *     last call's contents (each call clears the parts that must start at
+ *     zero).  Two calls whose GPU work overlapped would race on it, so calls
+ *     from several host threads of one process are serialised per device
+ *     inside the library (a call holds a lock until its stream has drained);
+ *     calls from other processes use their own copy. */
 #define CHIMERA_NOALLOC_MAX_CELLS 65536
 int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, double* Momx, double* Momy,
                              double* Energy, double* b_x, double* b_y, double* t,

@@ -8,9 +8,10 @@ _interp_to_grid does (test_validation.py:112-131), and stored as float32 (the
 file's values are single-precision data).  Run in an environment that has the
 reference checkout:
 
-    python tests/golden/make_ot_athena.py [path/to/ot_reference.h5]
+    python tests/golden/make_ot_athena.py path/to/ot_reference.h5
 
-(default: DEFAULT_SRC, where the build container keeps the reference checkout).
+or with CHIMERA_REFERENCE_DIR set to the root of the reference checkout (the
+file is then $CHIMERA_REFERENCE_DIR/tests/validation/ot_reference.h5).
 """
 import hashlib
 import os
@@ -22,7 +23,13 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspa
 from tests.golden.h5read import read_h5  # noqa: E402
 
 PINNED_SHA256 = "45e66217f6a81bae0831f8201b0cf6b10cdd75df3b5ecfd24c1e7899b5e92b5d"
-DEFAULT_SRC = "/root/reference/tests/validation/ot_reference.h5"
+
+def default_src():
+    """The pinned file inside the reference checkout named by
+    CHIMERA_REFERENCE_DIR, or None where that variable is unset."""
+    root = os.environ.get("CHIMERA_REFERENCE_DIR")
+    return os.path.join(root, "tests", "validation", "ot_reference.h5") if root else None
+
 GRIDS = (64, 128, 256)
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ot_athena_t05.npz")
 
@@ -61,4 +68,7 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC)
+    src = sys.argv[1] if len(sys.argv) > 1 else default_src()
+    if not src:
+        raise SystemExit("usage: make_ot_athena.py path/to/ot_reference.h5 (or set CHIMERA_REFERENCE_DIR)")
+    main(src)

@@ -9,7 +9,7 @@ import pytest
 
 from tests.golden import make_ot_athena as M
 
-SRC = M.DEFAULT_SRC   # the fixture script's source file (the reference checkout, where present)
+SRC = M.default_src()   # the fixture's source file, where CHIMERA_REFERENCE_DIR names the reference checkout
 
 
 def test_fixture_shapes():
@@ -21,7 +21,8 @@ def test_fixture_shapes():
             assert a.shape == (n, n) and np.all(a > 0)
 
 
-@pytest.mark.skipif(not os.path.exists(SRC), reason="reference checkout not present")
+@pytest.mark.skipif(not SRC or not os.path.exists(SRC),
+                    reason="CHIMERA_REFERENCE_DIR does not name a reference checkout")
 def test_fixture_reproduced_from_pinned_file():
     with open(SRC, "rb") as f:
         assert hashlib.sha256(f.read()).hexdigest() == M.PINNED_SHA256

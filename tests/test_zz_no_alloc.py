@@ -136,3 +136,77 @@ def test_noalloc_two_host_threads_are_serialised():
         for call in range(4):
             for q in range(6):
                 assert np.array_equal(results[k][call][q], wants[k][call][q]), (k, call, q)
+
+
+def test_noalloc_at_t_end_leaves_everything_untouched():
+    """A call with t >= t_end takes no step (the reference's loop has ended):
+    the six arrays, t, output_count and dt_next must come back bit for bit as
+    they went in -- not the scratch's contents."""
+    import torch
+    G = require_gpu()
+    step = _noalloc(G)
+    cfg, st = P.rotor(64, riemann=HLLE)
+    # run the scratch with another state first, so stale contents would show
+    other = [torch.from_numpy(a.copy()).cuda() for a in P.orszag_tang(64)[1]]
+    ocfg = G.to_ccfg(P.orszag_tang(64)[0])
+    t0, oc0 = C.c_double(0.0), C.c_int(1)
+    assert step(C.byref(ocfg), *[C.c_void_p(x.data_ptr()) for x in other], C.byref(t0), C.byref(oc0),
+                None, None) == 0
+    ccfg = G.to_ccfg(cfg)
+    for t_start in (cfg.t_end, cfg.t_end + 0.25):
+        dev = [torch.from_numpy(a.copy()).cuda() for a in st]
+        torch.cuda.synchronize()
+        t, oc, dtn = C.c_double(t_start), C.c_int(3), C.c_double(-7.5)
+        rc = step(C.byref(ccfg), *[C.c_void_p(x.data_ptr()) for x in dev], C.byref(t), C.byref(oc),
+                  C.byref(dtn), None)
+        assert rc == 0, G.lib().chimera_strerror(rc)
+        for q in range(6):
+            assert np.array_equal(dev[q].cpu().numpy(), st[q]), q
+        assert t.value == t_start and oc.value == 3 and dtn.value == -7.5
+
+
+def test_noalloc_rejects_nonpositive_t_end():
+    import torch
+    G = require_gpu()
+    step = _noalloc(G)
+    cfg, st = P.orszag_tang(16)
+    dev = [torch.from_numpy(a.copy()).cuda() for a in st]
+    torch.cuda.synchronize()
+    for t_end in (0.0, -1.0):
+        bad = G.to_ccfg(cfg.replace(t_end=t_end))
+        t, oc = C.c_double(0.0), C.c_int(1)
+        assert step(C.byref(bad), *[C.c_void_p(x.data_ptr()) for x in dev], C.byref(t), C.byref(oc),
+                    None, None) == -1
+    for q in range(6):
+        assert np.array_equal(dev[q].cpu().numpy(), st[q]), q
+
+
+def test_noalloc_step_clipped_by_output_time():
+    """A step that starts just before an output time: the dt is clipped to it
+    (src/main.f90:82-83) and output_count advances.  State, t, output_count
+    and the next dt equal the handle path's after chimera_set_time."""
+    import torch
+    G = require_gpu()
+    step = _noalloc(G)
+    cfg, st = P.orszag_tang(64, riemann=RUSANOV)
+    cfg = cfg.replace(t_out=0.05, t_end=0.5)
+    ccfg = G.to_ccfg(cfg)
+    t_start = 0.05 - 1.0e-4       # well inside one CFL step of the output time
+    ref = G.Solver(cfg)
+    ref.set_state(st)
+    ref.set_time(t_start, 1)
+    dev = [torch.from_numpy(a.copy()).cuda() for a in st]
+    torch.cuda.synchronize()
+    t, oc, dtn = C.c_double(t_start), C.c_int(1), C.c_double(0.0)
+    for call in range(2):
+        rc = step(C.byref(ccfg), *[C.c_void_p(x.data_ptr()) for x in dev], C.byref(t), C.byref(oc),
+                  C.byref(dtn), None)
+        assert rc == 0, G.lib().chimera_strerror(rc)
+        ref.step(1)
+        want = ref.get_state()
+        d = ref.diag()
+        for q in range(6):
+            assert np.array_equal(dev[q].cpu().numpy(), want[q]), (call, q)
+        assert t.value == d["t"] and oc.value == d["output_count"] and dtn.value == d["dt"]
+    assert oc.value == 2 and t.value > 0.05   # the first call landed on the output time
+    ref.close()
