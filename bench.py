@@ -64,6 +64,9 @@ def parse():
     p.add_argument("--slabs", type=int, default=0,
                    help="also run the FP64 Kelvin-Helmholtz grid as this many y-slabs on one GPU "
                         "(ghost-row exchange by device copies) against the undivided grid (0: off)")
+    p.add_argument("--ref-seconds", type=float, default=10.0,
+                   help="seconds of CPU work per timed sample of the CPU restatement (reference arm and "
+                        "cpu_baseline)")
     p.add_argument("--variant", type=int, default=-1,
                    help="force a tile variant for the single-grid measurement (-1: autotune)")
     return p.parse_args()
@@ -246,10 +249,28 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_reference_rate(n, steps, max_seconds=30.0, omp_mode=2):
+def cpu_model():
+    """The host CPU's model name (first /proc/cpuinfo entry), or the platform's."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_reference_rate(n, repeats=3, seconds=10.0, omp_mode=2):
     """The CPU restatement of the reference on the same workload, all host
-    threads: zone-cycles/s over a bounded sample.  omp_mode 2 threads every
-    loop; 1 threads only the three loops the reference threads."""
+    threads: zone-cycles/s of ``repeats`` timed samples of at least
+    ``seconds`` each, all from one warm state (two untimed steps first).  Each
+    sample is one oracle call of k steps, k calibrated from one timed step, so
+    the per-call set-up of the oracle's work arrays is amortised.  omp_mode 2
+    threads every loop; 1 threads only the three loops the reference threads.
+    Returns a dict with the median rate, the spread, the per-sample rates, the
+    cores used and the CPU model."""
     from chimera_b200 import problems
     from oracle import oracle
     oracle.build()
@@ -260,32 +281,44 @@ def cpu_reference_rate(n, steps, max_seconds=30.0, omp_mode=2):
     cfg, st = problems.rotor(n)
     cfg = cfg.replace(t_end=1e30)
     s = oracle.State(st)
-    oracle.run(cfg, s, 1)                      # warm-up (page-in, thread start)
-    done, t0 = 0, time.perf_counter()
-    while done < steps:
-        oracle.run(cfg, s, 1)
-        done += 1
-        if time.perf_counter() - t0 > max_seconds:
-            break
-    el = time.perf_counter() - t0
+    oracle.run(cfg, s, 2)                      # warm-up (page-in, thread start)
+    t0 = time.perf_counter()
+    oracle.run(cfg, s, 1)                      # calibration step
+    t1 = time.perf_counter() - t0
+    k = max(1, int(seconds / max(t1, 1e-6) + 0.999))
+    rates, steps, total = [], 0, 0.0
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        oracle.run(cfg, s, k)
+        el = time.perf_counter() - t0
+        rates.append(n * n * k / el)
+        steps += k
+        total += el
     cores = oracle.max_threads()
     oracle.set_omp_mode(0)
-    return n * n * done / el, cores, done, el
+    med = statistics.median(rates)
+    return {"value": med, "rates": rates, "spread": (max(rates) - min(rates)) / med, "cores": cores,
+            "steps": steps, "seconds": total, "steps_per_sample": k, "cpu_model": cpu_model(),
+            "ms_per_step": 1e3 * n * n / med}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    rate, cores, done, el = cpu_reference_rate(args.n, max(1, args.steps))
+    # --steps sets the number of timed samples (at least 3, each >= 10 s of CPU work)
+    r = cpu_reference_rate(args.n, repeats=max(3, min(args.steps, 5)), seconds=args.ref_seconds)
+    rate = r["value"]
     line = {
         "impl": "reference",
         "metric": "zone-cycles/s", "value": rate, "unit": "zone-cycles/s", "n_gpus": args.gpus,
-        "steps": done, "warmup": 1, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+        "steps": r["steps"], "warmup": 3, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD.replace("FP64 plain", "FP64, CPU"), "cells": args.n * args.n},
-        "cpu_baseline": {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "port",
-                         "sample": f"{done} RK3 steps of the {args.n}^2 rotor from t=0 (FP64 C restatement "
-                                   f"of the reference Fortran, OpenMP on every loop)"},
+        "cpu_baseline": {"value": rate, "unit": "zone-cycles/s", "cores": r["cores"], "kind": "port",
+                         "cpu_model": r["cpu_model"], "spread": r["spread"], "rates": r["rates"],
+                         "sample": f"median of {len(r['rates'])} samples of {r['steps_per_sample']} RK3 steps "
+                                   f"({r['seconds']:.1f} s in all) of the {args.n}^2 rotor from one warm state "
+                                   f"(FP64 C restatement of the reference Fortran, OpenMP on every loop)"},
         "e2e": {"value": rate, "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -396,15 +429,18 @@ def run_chimera(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, done, el = cpu_reference_rate(n, 4, max_seconds=20.0)
-        rate1, _, done1, el1 = cpu_reference_rate(n, 2, max_seconds=15.0, omp_mode=1)
-        cpu = {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "port",
-               "sample": f"{done} RK3 steps of the {n}^2 rotor from t=0 on the host cores "
-                         f"(FP64 C restatement, OpenMP on every loop), {el:.1f} s",
+        r = cpu_reference_rate(n, repeats=3, seconds=args.ref_seconds)
+        r1 = cpu_reference_rate(n, repeats=3, seconds=args.ref_seconds, omp_mode=1)
+        cpu = {"value": r["value"], "unit": "zone-cycles/s", "cores": r["cores"], "kind": "port",
+               "cpu_model": r["cpu_model"], "spread": r["spread"], "rates": r["rates"],
+               "sample": f"median of {len(r['rates'])} samples of {r['steps_per_sample']} RK3 steps "
+                         f"({r['seconds']:.1f} s in all) of the {n}^2 rotor from one warm state on the host "
+                         f"cores (FP64 C restatement, OpenMP on every loop)",
                "reference_threading": {
-                   "value": rate1, "unit": "zone-cycles/s",
-                   "sample": f"{done1} RK3 steps, OpenMP only on the three loops the reference "
-                             f"threads (src/mhd_derivatives.f90), {el1:.1f} s"}}
+                   "value": r1["value"], "unit": "zone-cycles/s", "spread": r1["spread"], "rates": r1["rates"],
+                   "sample": f"median of {len(r1['rates'])} samples of {r1['steps_per_sample']} RK3 steps, "
+                             f"OpenMP only on the three loops the reference threads "
+                             f"(src/mhd_derivatives.f90:79,105,186)"}}
 
     if rank == 0:
         line = {

@@ -9,7 +9,7 @@ import subprocess
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ARGS = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"]
+ARGS = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1", "--ref-seconds", "0.5"]
 
 
 def _lines(out):
@@ -25,6 +25,7 @@ def _check(line, n_gpus):
     cb = line["cpu_baseline"]
     assert cb["value"] == line["value"] and cb["kind"] == "port" and cb["sample"]
     assert cb["cores"] == len(os.sched_getaffinity(0))
+    assert len(cb["rates"]) >= 3 and cb["spread"] >= 0 and cb["cpu_model"]
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
 
