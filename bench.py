@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--ens-steps", type=int, default=200)
     p.add_argument("--ens-variant", type=int, default=-1,
                    help="force a tile variant for the FP32-batched ensemble (-1: autotune)")
-    p.add_argument("--ens-forms", default="fp32,fp64",
+    p.add_argument("--ens-forms", default="fp32,fp32mixed,fp64",
                    help="ensemble forms to measure (the L1 comparison needs both)")
     p.add_argument("--kh", choices=("on", "off"), default="on",
                    help="also measure the Kelvin-Helmholtz HLLD comparison (FP32-bulk vs FP64)")
@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--kh-steps", type=int, default=1000)
     p.add_argument("--adjoint", choices=("on", "off"), default="on",
                    help="also measure the field-loop adjoint (forward + backward, central differences)")
+    p.add_argument("--adj-steps", type=int, default=400, help="RK3 steps of the field-loop adjoint leg")
+    p.add_argument("--adj-k", type=int, default=20, help="checkpoint interval of the adjoint leg")
     p.add_argument("--slabs", type=int, default=0,
                    help="also run the FP64 Kelvin-Helmholtz grid as this many y-slabs on one GPU "
                         "(ghost-row exchange by device copies) against the undivided grid (0: off)")
@@ -476,14 +478,15 @@ def run_chimera(args, world, rank, local):
 
 def run_ensemble(args, world):
     """The batched GRF ensemble (one persistent launch per stage over all
-    members of uneven sizes, CUDA-graph replay) in the FP32-bulk form and in the
-    plain FP64 form from the same seeded states.  The FP64 GPU form reproduces
-    the FP64 oracle bit for bit (tests/test_gpu_parity.py, test_gpu_batch.py),
-    so the FP32 form's L1 error is measured against it on the full ensemble."""
+    members of uneven sizes, CUDA-graph replay) in the FP32-bulk form, the
+    FP32-arithmetic form on FP64 storage and the plain FP64 form from the same
+    seeded states.  The FP64 GPU form reproduces the FP64 oracle bit for bit
+    (tests/test_gpu_parity.py, test_gpu_batch.py), so the FP32 forms' L1 errors
+    are measured against it on the full ensemble, in all and per member size."""
     import numpy as np
     import torch
     from chimera_b200 import ensemble
-    from chimera_b200.config import FP32_BULK, FP64
+    from chimera_b200.config import FP32_BULK, FP32_MIXED, FP64
 
     from chimera_b200 import problems
     from chimera_b200.shard import shard_members
@@ -497,7 +500,8 @@ def run_ensemble(args, world):
     sizes = problems.grf_ensemble_sizes(args.ens_scale)
     all_cells = sum(n * n for n in sizes)
     mine = set(shard_members([n * n for n in sizes], world, rank))   # members are independent: no exchange
-    forms = [(n, p) for n, p in (("fp32_batched", FP32_BULK), ("fp64_batched", FP64))
+    forms = [(n, p) for n, p in (("fp32_batched", FP32_BULK), ("fp32mixed_batched", FP32_MIXED),
+                                 ("fp64_batched", FP64))
              if n.split("_")[0] in args.ens_forms.split(",")]
     for name, prec in forms:
         cfgs, states = ensemble.grf_ensemble(args.ens_scale, prec, members=mine)
@@ -530,6 +534,7 @@ def run_ensemble(args, world):
         e1.synchronize()
         ms = dist_max(e0.elapsed_time(e1), world)
         esize = 4 if prec == FP32_BULK else 8
+        member_sizes = [c.nx for c in cfgs]
         zcs = cells * steps / (ms * 1e-3)
         res[name] = {"value": zcs, "unit": "zone-cycles/s", "ms": ms, "steps": steps,
                      "members": len(sizes), "members_per_rank_max": len(cfgs), "cells": cells,
@@ -553,10 +558,12 @@ def run_ensemble(args, world):
     if "fp32_batched" not in finals or "fp64_batched" not in finals:
         return res
 
-    def l1_vs_fp64(key):
+    def l1_vs_fp64(key, size=None):
         num = np.zeros(6)
         den = np.zeros(6)
-        for a, b in zip(finals[key], finals["fp64_batched"]):
+        for n, a, b in zip(member_sizes, finals[key], finals["fp64_batched"]):
+            if size is not None and n != size:
+                continue
             for q in range(6):
                 num[q] += np.sum(np.abs(a[q] - b[q]))
                 den[q] += np.sum(np.abs(b[q]))
@@ -565,11 +572,19 @@ def run_ensemble(args, world):
             t = torch.tensor(np.concatenate([num, den]), dtype=torch.float64, device="cuda")
             dist.all_reduce(t)
             num, den = t[:6].cpu().numpy(), t[6:].cpu().numpy()
-        return dict(zip(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y"), (num / den).tolist()))
+        return dict(zip(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y"), (num / np.maximum(den, 1e-300)).tolist()))
 
     res["fp32_l1_vs_fp64"] = l1_vs_fp64("fp32_batched")
     res["fp64_from_fp32_rounded_ic_l1_vs_fp64"] = l1_vs_fp64("fp64_ic_rounded")
     res["fp32_over_fp64"] = res["fp32_batched"]["value"] / res["fp64_batched"]["value"]
+    sizes_present = sorted(set(sizes))
+    res["l1_vs_fp64_by_member_size"] = {
+        key: {str(n): max(l1_vs_fp64(k, n).values()) for n in sizes_present}
+        for key, k in (("fp32_bulk", "fp32_batched"), ("fp32_mixed", "fp32mixed_batched"),
+                       ("fp64_from_fp32_rounded_ic", "fp64_ic_rounded")) if k in finals}
+    if "fp32mixed_batched" in finals:
+        res["fp32mixed_l1_vs_fp64"] = l1_vs_fp64("fp32mixed_batched")
+        res["fp32mixed_over_fp64"] = res["fp32mixed_batched"]["value"] / res["fp64_batched"]["value"]
     res["workload"] = (f"GRF ensemble, {res['fp32_batched']['members']} members of uneven sizes "
                        f"(128^2/256^2/512^2), periodic, Rusanov + MC + MOOD, {steps} RK3 steps")
     return res
@@ -593,16 +608,17 @@ def _timed_run(s, steps, graph):
 
 def run_kh(args):
     """Kelvin-Helmholtz n^2 on [0,1]x[-1,1] (HLLD + MC + MOOD), the FP32-bulk
-    form against the plain FP64 form on the same GPU from the same state:
-    zone-cycles/s of each (graph replay), L1 error per field and div B."""
+    form and the FP32-arithmetic form on FP64 storage against the plain FP64
+    form on the same GPU from the same state: zone-cycles/s of each (graph
+    replay), L1 error per field and div B."""
     import numpy as np
     from chimera_b200 import gpu, problems
-    from chimera_b200.config import FP32_BULK, FP64
+    from chimera_b200.config import FP32_BULK, FP32_MIXED, FP64
     n, steps = args.kh_n, args.kh_steps
     graph = 10 if steps % 10 == 0 else 1
     cfg, st = problems.kelvin_helmholtz(n)
     res, finals = {}, {}
-    for name, prec in (("fp32_bulk", FP32_BULK), ("fp64", FP64)):
+    for name, prec in (("fp32_bulk", FP32_BULK), ("fp32_mixed", FP32_MIXED), ("fp64", FP64)):
         s = gpu.Solver(cfg.replace(precision=prec))
         s.set_state(st)
         s.autotune(reps=1)
@@ -617,12 +633,14 @@ def run_kh(args):
         res[name] = {"value": n * n * steps / (ms * 1e-3), "unit": "zone-cycles/s", "ms": ms,
                      "divb_rel": d["divb_rel"], "tile": s.variant()}
         s.close()
-    l1 = {}
-    for q, f in enumerate(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y")):
-        a, b = finals["fp32_bulk"][q], finals["fp64"][q]
-        l1[f] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
-    res["fp32_l1_vs_fp64"] = l1
+    for key, form in (("fp32_l1_vs_fp64", "fp32_bulk"), ("fp32mixed_l1_vs_fp64", "fp32_mixed")):
+        l1 = {}
+        for q, f in enumerate(("Mass", "Momx", "Momy", "Energy", "b_x", "b_y")):
+            a, b = finals[form][q], finals["fp64"][q]
+            l1[f] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+        res[key] = l1
     res["fp32_over_fp64"] = res["fp32_bulk"]["value"] / res["fp64"]["value"]
+    res["fp32mixed_over_fp64"] = res["fp32_mixed"]["value"] / res["fp64"]["value"]
     res["workload"] = (f"Kelvin-Helmholtz {n}^2 on [0,1]x[-1,1], periodic, HLLD + MC + MOOD, gamma 1.4, "
                        f"{steps} RK3 steps from the same state")
     return res
@@ -684,8 +702,8 @@ def run_adjoint_leg(args):
     import numpy as np
     import torch
     from chimera_b200 import adjoint, problems
-    from chimera_b200.config import HLLE, VAN_LEER
-    n, steps, K = 512, 400, 20
+    from chimera_b200.config import FP32_BULK, FP32_MIXED, FP64, HLLE, VAN_LEER
+    n, steps, K = 512, args.adj_steps, args.adj_k
     cfg, st = problems.field_loop(n, n, 2.0, 1.0, v=(2.0, 1.0), riemann=HLLE, limiter=VAN_LEER)
     vol = cfg.dx * cfg.dy
     M, Mx, My, E, bx, by = st
@@ -697,13 +715,13 @@ def run_adjoint_leg(args):
     dts = adjoint.cfl_dts(cfg, U0, steps)
     adj = adjoint.Adjoint(cfg)
 
-    def loss_of(pr, grad):
+    def loss_of(pr, grad, precision=FP64):
         U = [u.contiguous() for u in adjoint.conserved_from_primitive(cfg, *pr)]
         if not grad:
             for dt in dts:
                 U = adj.forward_step(U, dt)
             return adjoint.magnetic_energy(cfg, U)
-        return adjoint.magnetic_energy(cfg, adjoint.run(adj, U, dts, K=K))
+        return adjoint.magnetic_energy(cfg, adjoint.run(adj, U, dts, K=K, precision=precision))
 
     with torch.no_grad():
         loss_of(prims, False)                           # warm-up
@@ -738,11 +756,30 @@ def run_adjoint_leg(args):
         fd = (lp - lm) / (2 * eps)
         an = sum(float(torch.sum(g_in[k].grad * dirs[k])) for k in range(3))
         worst = max(worst, abs(fd - an) / abs(an))
-    return {"workload": "field-loop adjoint 512^2 on [0,2]x[0,1], v = (2, 1), HLLE + Van Leer, 400 RK3 steps, "
-                        "K = 20, loss = final magnetic energy, gradient w.r.t. initial rho, vx, vy",
+    # the forward in the reduced-precision forms (fused FP32 solver, same frozen dts),
+    # the adjoint in FP64 from their checkpoints
+    forms = {}
+    g64 = [g_in[k].grad for k in range(3)]
+    for name, prec in (("fp32_bulk", FP32_BULK), ("fp32_mixed", FP32_MIXED)):
+        gp = [x.clone().requires_grad_(k < 3) for k, x in enumerate(prims)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lossp = loss_of(gp, True, prec)
+        torch.cuda.synchronize()
+        t_f = time.perf_counter() - t0
+        lossp.backward()
+        torch.cuda.synchronize()
+        t_all = time.perf_counter() - t0
+        rel = max(float(torch.max(torch.abs(gp[k].grad - g64[k])) / torch.max(torch.abs(g64[k]))) for k in range(3))
+        forms[name] = {"forward_s": t_f, "forward_backward_s": t_all, "loss": float(lossp),
+                       "loss_rel_vs_fp64": abs(float(lossp) - base) / abs(base),
+                       "gradient_max_rel_vs_fp64_forward": rel}
+    return {"workload": f"field-loop adjoint 512^2 on [0,2]x[0,1], v = (2, 1), HLLE + Van Leer, {steps} RK3 steps, "
+                        f"K = {K}, loss = final magnetic energy, gradient w.r.t. initial rho, vx, vy",
             "forward_s": t_fwd, "forward_backward_s": t_fb, "loss": base,
             "gradient_zone_cycles_per_s": n * n * steps / t_fb,
             "central_difference_rel_err_2_dirs": worst,
+            "reduced_precision_forward": forms,
             "note": "rho and v start exactly uniform, so every rho / v limiter starts at its kink: central "
                     "differences agree with the stated one-sided convention to about 3e-3 here, and to 1e-6 "
                     "on a generic state (tests/test_gpu_adjoint.py)"}

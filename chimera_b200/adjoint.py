@@ -11,7 +11,16 @@ function of the state, so the derivative of the CFL reduction is not taken;
 obtain the dt sequence from a primal run (``cfl_dts``) and reuse it.  The MOOD,
 floor and thermal-check decisions and the limiter branches are the forward's;
 at a kink the derivative is that of the branch the forward took (one-sided).
-Periodic boundaries, FP64.
+Periodic boundaries.
+
+Forward precision: FP64 (the tape kernels, bit-identical to the fused FP64
+step) or a reduced form -- ``FP32_BULK`` or ``FP32_MIXED`` -- in which the
+forward steps run through the fused FP32 solver with the same frozen time
+steps (``chimera_set_dt_device`` before each step) and the loss is the
+reduced-precision result.  The checkpoints are that forward's states (as FP64);
+backward re-runs each segment from its checkpoint in FP64 and applies the FP64
+adjoint, so the gradient is the FP64 adjoint along the reduced-precision
+trajectory, restarted from it every K steps.
 """
 from __future__ import annotations
 
@@ -20,7 +29,7 @@ import ctypes as C
 import torch
 
 from . import gpu
-from .config import FP64, SolverConfig
+from .config import FP32_BULK, FP32_MIXED, FP64, SolverConfig
 
 _bound = False
 
@@ -105,17 +114,46 @@ def cfl_dts(cfg: SolverConfig, U, nsteps: int):
     return dts
 
 
+def _forward_reduced(cfg: SolverConfig, U0, dts, K: int, precision: int):
+    """The forward steps in a reduced-precision form with the given time steps:
+    (checkpoints every K steps as FP64 tensors, final state as FP64 tensors)."""
+    # t_end / t_out far away: every step is taken with the dt given (the CFL
+    # dt the solver computes after each step is overwritten before the next)
+    c = cfg.replace(precision=precision, t_end=1.0e300, t_out=1.0e300)
+    dt_dev = torch.tensor([float(d) for d in dts], dtype=torch.float64, device=U0[0].device)
+    torch.cuda.current_stream().synchronize()   # the solver's own stream reads U0 and dt_dev
+    checkpoints = [(0, [u.clone() for u in U0])]
+    with gpu.Solver(c) as s:
+        s.set_state(U0)
+        for i in range(len(dts)):
+            s.set_dt_device(dt_dev[i:i + 1])
+            s.step(1)
+            if (i + 1) % K == 0 and i + 1 < len(dts):
+                ck = [torch.empty_like(u) for u in U0]
+                s.get_state(out=ck)
+                checkpoints.append((i + 1, ck))
+        final = [torch.empty_like(u) for u in U0]
+        s.get_state(out=final)
+    return checkpoints, final
+
+
 class RK3Run(torch.autograd.Function):
-    """U_N = RK3^N(U_0) with frozen dts; checkpoints every K steps."""
+    """U_N = RK3^N(U_0) with frozen dts; checkpoints every K steps; forward
+    in FP64 or a reduced-precision form (module docstring)."""
 
     @staticmethod
-    def forward(ctx, adj: Adjoint, dts, K: int, *U0):
+    def forward(ctx, adj: Adjoint, dts, K: int, precision: int, *U0):
         U = [u.detach().contiguous() for u in U0]
-        checkpoints = [(0, [u.clone() for u in U])]
-        for s, dt in enumerate(dts):
-            U = adj.forward_step(U, dt)
-            if (s + 1) % K == 0 and s + 1 < len(dts):
-                checkpoints.append((s + 1, [u.clone() for u in U]))
+        if precision == FP64:
+            checkpoints = [(0, [u.clone() for u in U])]
+            for s, dt in enumerate(dts):
+                U = adj.forward_step(U, dt)
+                if (s + 1) % K == 0 and s + 1 < len(dts):
+                    checkpoints.append((s + 1, [u.clone() for u in U]))
+        elif precision in (FP32_BULK, FP32_MIXED):
+            checkpoints, U = _forward_reduced(adj.cfg, U, dts, K, precision)
+        else:
+            raise ValueError(f"unknown forward precision {precision}")
         ctx.adj = adj
         ctx.dts = list(dts)
         ctx.K = K
@@ -138,12 +176,13 @@ class RK3Run(torch.autograd.Function):
                 states.append(adj.forward_step(states[-1], dts[s]))
             for s in range(end - 1, start - 1, -1):
                 lam = adj.step_vjp(states[s - start], dts[s], lam)
-        return (None, None, None, *lam)
+        return (None, None, None, None, *lam)
 
 
-def run(adj: Adjoint, U0, dts, K: int = 20):
-    """Differentiable RK3 run (see RK3Run)."""
-    return RK3Run.apply(adj, list(dts), int(K), *U0)
+def run(adj: Adjoint, U0, dts, K: int = 20, precision: int = FP64):
+    """Differentiable RK3 run (see RK3Run); ``precision`` is the forward's
+    (FP64, FP32_BULK or FP32_MIXED); the adjoint is FP64."""
+    return RK3Run.apply(adj, list(dts), int(K), int(precision), *U0)
 
 
 # --- helpers for losses on primitive inputs ------------------------------------

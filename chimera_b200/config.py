@@ -20,6 +20,8 @@ BC_PERIODIC, BC_FIXED, BC_OUTFLOW, BC_INFLOW = 1, 2, 3, 4
 # precision forms of the GPU path
 FP64 = 0        # plain FP64, bit-compatible with the FP64 restatement
 FP32_BULK = 1   # FP32 storage and bulk arithmetic; FP64 pressure recovery, dt and sums
+FP32_MIXED = 2  # FP64 storage; FP32 reconstruction / limiter / MOOD / Riemann arithmetic; FP64 pressure
+                # recovery, updates, floors, RK blends, dt and sums
 
 
 @dataclass

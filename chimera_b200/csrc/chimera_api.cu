@@ -73,17 +73,20 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Tensor map of one FP32 (ny, nx) field with a bw x bh box; false if the
-// field's shape does not allow one (row pitch not a multiple of 16 bytes, or
-// smaller than the box).
-bool encode_field_map(void* map, void* base, int nx, int ny, int bw, int bh) {
+// Tensor map of one (ny, nx) field of FP32 (elem 4) or FP64 (elem 8) values
+// with a bw x bh box; false if the field's shape does not allow one (row pitch
+// not a multiple of 16 bytes, or smaller than the box).
+bool encode_field_map(void* map, void* base, int nx, int ny, int bw, int bh, int elem) {
   EncodeTiledFn fn = encode_tiled();
-  if (!fn || nx % 4 != 0 || nx < bw || ny < bh || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  if (!fn || (size_t(nx) * elem) % 16 != 0 || (size_t(bw) * elem) % 16 != 0 || nx < bw || ny < bh ||
+      (reinterpret_cast<uintptr_t>(base) & 15) != 0)
+    return false;
   const cuuint64_t dims[2] = {cuuint64_t(nx), cuuint64_t(ny)};
-  const cuuint64_t strides[1] = {cuuint64_t(nx) * sizeof(float)};
+  const cuuint64_t strides[1] = {cuuint64_t(nx) * cuuint64_t(elem)};
   const cuuint32_t box[2] = {cuuint32_t(bw), cuuint32_t(bh)};
   const cuuint32_t estr[2] = {1, 1};
-  return fn(static_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+  const CUtensorMapDataType dt = (elem == 8) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(static_cast<CUtensorMap*>(map), dt, 2, base, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -160,7 +163,8 @@ static int validate_cfg(const chimera_cfg* c) {
   if ((c->bc_ylo == CHIMERA_BC_PERIODIC) != (c->bc_yhi == CHIMERA_BC_PERIODIC)) return CHIMERA_ERR_UNSUPPORTED;
   if (c->riemann < 1 || c->riemann > 3) return CHIMERA_ERR_BAD_ARG;
   if (c->limiter < 1 || c->limiter > 2) return CHIMERA_ERR_BAD_ARG;
-  if (c->precision != CHIMERA_FP64 && c->precision != CHIMERA_FP32_BULK) return CHIMERA_ERR_BAD_ARG;
+  if (c->precision != CHIMERA_FP64 && c->precision != CHIMERA_FP32_BULK && c->precision != CHIMERA_FP32_MIXED)
+    return CHIMERA_ERR_BAD_ARG;
   return CHIMERA_OK;
 }
 
@@ -437,11 +441,14 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
   h->precision = cfgs[0].precision;
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  const int nv = (h->precision == CHIMERA_FP64) ? fp64_variant_count() : fp32_variant_count();
+  const int nv = (h->precision == CHIMERA_FP64)       ? fp64_variant_count()
+                 : (h->precision == CHIMERA_FP32_BULK) ? fp32_variant_count()
+                                                       : fp32m_variant_count();
   h->variants.resize(nv);
   for (int v = 0; v < nv; ++v) {
     if (h->precision == CHIMERA_FP64) fp64_kernels(v, &h->variants[v]);
-    else fp32_kernels(v, &h->variants[v]);
+    else if (h->precision == CHIMERA_FP32_BULK) fp32_kernels(v, &h->variants[v]);
+    else fp32m_kernels(v, &h->variants[v]);
     for (int r = 0; r < 3; ++r)
       for (int st = 0; st < 3; ++st)
         cudaFuncSetAttribute(h->variants[v].stage[r][st].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -532,7 +539,7 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
         for (int b = 0; b < 3 && ok; ++b)
           for (int q = 0; q < 6 && ok; ++q)
             ok = encode_field_map(&maps[sl * per_slot + (size_t(m) * 18 + b * 6 + q) * TMAP_BYTES_HOST],
-                                  g.buf[b][q], g.nx, g.ny, bw, bh);
+                                  g.buf[b][q], g.nx, g.ny, bw, bh, h->variants[v].elem_bytes);
         h->tmap_ok[size_t(sl) * n_members + m] = ok ? 1 : 0;
       }
     }
@@ -605,7 +612,7 @@ static int copy_field_in(chimera_handle* h, int m, void* dst, const double* src,
   const chimera_cfg& c = h->cfg[m];
   const size_t w = size_t(c.nx) * sizeof(double);
   const cudaMemcpyKind kind = (where == CHIMERA_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-  if (h->precision == CHIMERA_FP64) {
+  if (h->ks.elem_bytes == 8) {   // FP64 storage
     CK(cudaMemcpy2DAsync(dst, w, src, size_t(ld) * sizeof(double), w, c.ny, kind, h->stream));
   } else {
     CK(cudaMemcpy2DAsync(h->d_stage64, w, src, size_t(ld) * sizeof(double), w, c.ny, kind, h->stream));
@@ -620,7 +627,7 @@ static int copy_field_out(chimera_handle* h, int m, double* dst, const void* src
   const chimera_cfg& c = h->cfg[m];
   const size_t w = size_t(c.nx) * sizeof(double);
   const cudaMemcpyKind kind = (where == CHIMERA_HOST) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  if (h->precision == CHIMERA_FP64) {
+  if (h->ks.elem_bytes == 8) {   // FP64 storage
     CK(cudaMemcpy2DAsync(dst, size_t(ld) * sizeof(double), src, w, w, c.ny, kind, h->stream));
   } else {
     const size_t n = cells_of(c);
@@ -843,6 +850,31 @@ int chimera_advance(chimera_handle* h, int max_steps, int* steps_taken) {
   for (int m = 0; m < h->n; ++m)
     if (c[m].status) return CHIMERA_ERR_NONFINITE;
   return CHIMERA_OK;
+}
+
+// Set (pause = true) or clear the pause-at-output flag of every member; a
+// member that paused is resumed (active again while t < t_end).
+static int set_pause(chimera_handle* h, bool pause) {
+  std::vector<Control> c(h->n);
+  CK(cudaMemcpyAsync(c.data(), h->d_ctl, sizeof(Control) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int m = 0; m < h->n; ++m) {
+    if (c[m].flags & CTL_PAUSED) c[m].active = (c[m].t < h->cfg[m].t_end) ? 1 : 0;
+    c[m].flags = pause ? CTL_PAUSE_AT_OUTPUT : 0;
+  }
+  CK(cudaMemcpyAsync(h->d_ctl, c.data(), sizeof(Control) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return CHIMERA_OK;
+}
+
+int chimera_advance_output(chimera_handle* h, int max_steps, int* steps_taken) {
+  NvtxRange range("chimera_advance_output");
+  if (!h || max_steps < 0) return CHIMERA_ERR_BAD_ARG;
+  int rc = set_pause(h, true);
+  if (rc) return rc;
+  rc = chimera_advance(h, max_steps, steps_taken);
+  const int rc2 = set_pause(h, false);   // on the error path too: no member stays paused
+  return rc ? rc : rc2;
 }
 
 int chimera_stage(chimera_handle* h, int k, double dt) {

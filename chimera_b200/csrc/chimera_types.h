@@ -7,6 +7,12 @@ namespace chimera {
 
 constexpr int NPART = 6;  // per-tile partials: cfl speed max, |divB| max, |divB| sum, |B| max, mass, energy
 
+// Control::flags
+enum : int {
+  CTL_PAUSE_AT_OUTPUT = 1,   // stop (active = 0) after the step that reaches an output time
+  CTL_PAUSED = 2,            // stopped there; the host resumes the member
+};
+
 enum : unsigned {
   STATUS_NONFINITE = 1u,   // a non-finite or non-positive quantity reached a reduction
   STATUS_TIMEOUT = 2u,     // a bounded wait gave up
@@ -42,7 +48,7 @@ struct Member {
 struct Control {
   double t, dt;
   int output_count, active;
-  int parity, pad0;        // buf[parity] holds the current state
+  int parity, flags;       // buf[parity] holds the current state; flags: CTL_*
   unsigned tiles_done, status;
   unsigned long long steps, mood_resets, floor_hits;
   double cfl_speed, divb_max, divb_sum, bmax, mass, energy;

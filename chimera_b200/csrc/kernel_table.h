@@ -23,5 +23,7 @@ int fp64_variant_count();
 void fp64_kernels(int variant, KernelSet* out);
 int fp32_variant_count();
 void fp32_kernels(int variant, KernelSet* out);
+int fp32m_variant_count();
+void fp32m_kernels(int variant, KernelSet* out);
 
 }  // namespace chimera

@@ -7,20 +7,22 @@
 namespace chimera {
 
 namespace {
-template <int TX, int TY, int NT, int MINB, bool SB = true, bool TMA = false>
+// Storage type ST: float (FP32-bulk) or double (FP32 arithmetic on FP64
+// storage, whose dt comes from the FP64 CFL kernel, as its epilogue's does).
+template <int TX, int TY, int NT, int MINB, bool SB = true, bool TMA = false, typename ST = float>
 void fill(KernelSet* ks) {
   using G = TileGeom32<TX, TY, SB>;
   const size_t smem = G::smem_bytes();
   const int bw = TMA ? G::BW : 0, bh = TMA ? G::BH : 0;
 #define CHIMERA_ENTRY(S, K)                                                                            \
   ks->stage[S - 1][K - 1] =                                                                           \
-      KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB, TMA>, smem, TX, TY, NT, bw, bh}
+      KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB, TMA, ST>, smem, TX, TY, NT, bw, bh}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
 #undef CHIMERA_ENTRY
-  ks->cfl = KernelEntry{(const void*)&cfl_kernel<float, TX, TY, NT>, 0, TX, TY, NT};
-  ks->elem_bytes = 4;
+  ks->cfl = KernelEntry{(const void*)&cfl_kernel<ST, TX, TY, NT>, 0, TX, TY, NT};
+  ks->elem_bytes = int(sizeof(ST));
 }
 }  // namespace
 
@@ -40,6 +42,18 @@ void fp32_kernels(int variant, KernelSet* out) {
     case 9: fill<32, 16, 256, 3, false, true>(out); break;
     case 10: fill<16, 16, 128, 6, false, true>(out); break;
     default: fill<32, 16, 256, 2>(out); break;
+  }
+}
+
+// The FP32-arithmetic form on FP64 storage: the FP32-bulk tiles without TMA.
+int fp32m_variant_count() { return 4; }
+
+void fp32m_kernels(int variant, KernelSet* out) {
+  switch (variant) {
+    case 1: fill<32, 16, 256, 3, false, false, double>(out); break;
+    case 2: fill<32, 8, 128, 5, false, false, double>(out); break;
+    case 3: fill<16, 16, 128, 6, false, false, double>(out); break;
+    default: fill<32, 16, 256, 2, true, false, double>(out); break;
   }
 }
 

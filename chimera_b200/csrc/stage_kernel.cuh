@@ -22,6 +22,7 @@
 #pragma once
 #include "mhd_device.cuh"
 #include "chimera_types.h"
+#include "tma.cuh"
 
 namespace chimera {
 
@@ -66,6 +67,20 @@ template <int TX, int TY> struct TileGeom {
     return sizeof(R) * (size_t(6) * NP + size_t(5) * NFX + size_t(5) * NFY + NBX + NBY +
                         (KEEP_IN ? size_t(4) * TX * TY : 0));
   }
+};
+
+// TMA box of the FP64 stage input (variants with TMA): the six fields over
+// cells [i0-4, i0-4+BW) x [j0-3, j0-3+BH) -- the primitives' 2-cell halo plus
+// the face-B neighbours b_x(i-1), b_y(j-1) -- with the origin's x even (a
+// multiple of 16 bytes: TX is even), each field's box padded to 128 bytes.
+// The boxes land in the face-flux arrays, which phase 1 does not use.
+template <int TX, int TY> struct TmaBox64 {
+  static_assert(TX % 2 == 0, "the box origin i0 - 4 must be a multiple of 2 doubles");
+  static constexpr int BW = ((TX + 6 + 1) / 2) * 2;
+  static constexpr int BH = TY + 5;
+  static constexpr int BOXF = ((BW * BH + 15) / 16) * 16;
+  static constexpr bool FITS = 6 * BOXF + 16 <=
+                               5 * TileGeom<TX, TY>::NFX + 5 * TileGeom<TX, TY>::NFY;   // (+16: alignment slack)
 };
 
 // L2 prefetch of the input rows the CTA's NEXT tile (work item w_next) will
@@ -218,9 +233,13 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
   if (threadIdx.x == 0) {
     double t = ctl->t;
     int oc = ctl->output_count;
+    bool output_reached = false;
     if (advance_time) {
       t = t + ctl->dt;                                           // src/main.f90:273
-      if (t >= double(oc) * g.t_out || t >= g.t_end) oc += 1;    // src/main.f90:279,291
+      if (t >= double(oc) * g.t_out || t >= g.t_end) {           // src/main.f90:279,291
+        oc += 1;
+        output_reached = true;
+      }
       ctl->steps += 1;
       ctl->parity = 1 - ctl->parity;                             // U^{n+1} now in the other buffer
     }
@@ -233,6 +252,12 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
     ctl->output_count = oc;
     ctl->dt = dt;
     ctl->active = (t < g.t_end) ? 1 : 0;
+    // a run that stops at every output time pauses after the step that
+    // reached one -- where the reference writes its snapshot (src/main.f90:279-292)
+    if (output_reached && (ctl->flags & CTL_PAUSE_AT_OUTPUT)) {
+      ctl->active = 0;
+      ctl->flags |= CTL_PAUSED;
+    }
     ctl->cfl_speed = sp;
     ctl->divb_max = dmx;
     ctl->divb_sum = dsum;
@@ -259,7 +284,8 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
 // memory, and phase 3b reads them there instead of from L2 (16 KB more for a
 // 32 x 16 tile; fewer live registers through the update, and fewer spills).
 // ----------------------------------------------------------------------------
-template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool KEEP_IN = false>
+template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool KEEP_IN = false,
+          bool TMA = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   using G = TileGeom<TX, TY>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -273,11 +299,23 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   __shared__ int s_last;
   __shared__ unsigned s_own;   // stage 3: bit r set if tile row r is one of the grid's own rows
   static_assert(TY < 32, "the own-row mask holds one bit per tile row");
+  using BX = TmaBox64<TX, TY>;
+  static_assert(!TMA || (sizeof(R) == 8 && BX::FITS), "FP64 boxes in the face-flux arrays");
+  __shared__ __align__(8) uint64_t s_bar;   // TMA completion
+  __shared__ unsigned s_phase;              // parity of the mbarrier phase the next box completes
 
   const int tid = threadIdx.x;
   const bool slope_on = a.slope_limiting != 0;
   const bool mood_on = a.mood != 0;
   const bool van_leer = a.limiter == LIMITER_VAN_LEER;
+  constexpr unsigned TMA_POLLS = 1u << 26;   // bound of every wait for a TMA completion
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init(&s_bar, 1);
+      s_phase = 0u;
+    }
+    __syncthreads();
+  }
 
   for (int w = a.work_begin + blockIdx.x; w < a.total_tiles; w += gridDim.x) {
     const int m = (a.n_members == 1) ? 0 : a.tile_member[w];
@@ -308,7 +346,62 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     // (src/mhd_change_states.f90:61-113).  Out-of-domain positions take the
     // primitive of the cell that fill_ghost_cells would copy there
     // (src/mhd_bc.f90:36-121): wrap if periodic, else the nearest cell.
-    {
+    // TMA variants: a tile whose box lies inside the arrays (no index map
+    // applies: every position is a cell of the grid) reads its inputs from six
+    // box copies; the others take the plain loads below.
+    bool from_box = false;
+    if constexpr (TMA) {
+      from_box = g.tmap != nullptr && i0 >= 4 && i0 - 4 + BX::BW <= nx && j0 >= 3 && j0 - 3 + BX::BH <= ny;
+      if (from_box) {   // uniform across the CTA
+        const R* stg = reinterpret_cast<const R*>((reinterpret_cast<uintptr_t>(sFx) + 127) & ~uintptr_t(127));
+        if (tid == 0) {
+          // the previous tile's generic reads of these arrays (ordered before the
+          // loop's closing barrier) precede the async-proxy writes
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(&s_bar, unsigned(6 * BX::BW * BX::BH * sizeof(R)));
+          const char* maps = reinterpret_cast<const char*>(g.tmap) + size_t(in_buf) * 6 * TMAP_BYTES;
+#pragma unroll
+          for (int q = 0; q < 6; ++q)
+            tma_load_2d(const_cast<R*>(stg) + q * BX::BOXF, maps + q * TMAP_BYTES, i0 - 4, j0 - 3, &s_bar);
+        }
+        const bool ok = mbar_wait(&s_bar, s_phase, TMA_POLLS);
+        for (int p = tid; p < G::NP && ok; p += NT) {
+          const int qx = p % G::PX, qy = p / G::PX;
+          const int b = (qy + 1) * BX::BW + (qx + 2);   // box element of cell (i0-2+qx, j0-2+qy)
+          const R Bx = R(0.5) * (stg[4 * BX::BOXF + b] + stg[4 * BX::BOXF + b - 1]);
+          const R By = R(0.5) * (stg[5 * BX::BOXF + b] + stg[5 * BX::BOXF + b - BX::BW]);
+          const R c0 = stg[b], c1 = stg[BX::BOXF + b], c2 = stg[2 * BX::BOXF + b], c3 = stg[3 * BX::BOXF + b];
+          if constexpr (KEEP_IN) {
+            const int ox = qx - 2, oy = qy - 2;
+            if (ox >= 0 && ox < TX && oy >= 0 && oy < TY) {
+              const int c = oy * TX + ox;
+              sU[0 * (TX * TY) + c] = c0;
+              sU[1 * (TX * TY) + c] = c1;
+              sU[2 * (TX * TY) + c] = c2;
+              sU[3 * (TX * TY) + c] = c3;
+            }
+          }
+          Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol);
+          sP[0 * G::NP + p] = pr.rho;
+          sP[1 * G::NP + p] = pr.vx;
+          sP[2 * G::NP + p] = pr.vy;
+          sP[3 * G::NP + p] = pr.P;
+          sP[4 * G::NP + p] = pr.Bx;
+          sP[5 * G::NP + p] = pr.By;
+        }
+        if (__syncthreads_or(!ok)) {   // a copy that never landed: status word, end the kernel
+          if (tid == 0) {
+            atomicOr(&ctl->status, STATUS_TIMEOUT);
+            // one more bounded wait for the copies in flight, with the CTA (and
+            // its shared memory) still resident, before it exits
+            mbar_wait(&s_bar, s_phase, TMA_POLLS);
+          }
+          return;
+        }
+        if (tid == 0) s_phase ^= 1u;   // every thread has read it (before the barrier above)
+      }
+    }
+    if (!from_box) {
       const R* __restrict__ in[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
@@ -344,7 +437,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         sP[5 * G::NP + p] = pr.By;
       }
     }
-    __syncthreads();
+    if (!from_box) __syncthreads();   // (the box path ended with its own barrier)
 
     // ---- phase 2: face fluxes ------------------------------------------------
     unsigned mood_resets = 0;

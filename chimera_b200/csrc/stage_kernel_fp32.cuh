@@ -19,6 +19,15 @@
 // Kept in FP64: the pressure recovery p = (gamma-1)(E - rho v^2/2 - B^2/2)
 // (get_primitive_mixed), the CFL dt reduction and the tOut clip, and the
 // conserved-total sums.  The per-cell CFL speed is computed in FP32.
+//
+// Storage type S: float for the FP32-bulk form.  With S = double (the
+// FP32-arithmetic form on FP64 storage) the state stays FP64 in HBM and only
+// the reconstruction, limiter, MOOD and Riemann arithmetic (phases 1.5 and 2,
+// and the corner Ez of phase 3a) run in FP32: the primitives are recovered in
+// FP64 (get_primitive, then rounded to FP32), and the face-B update, the cell
+// update, the outflow correction, the floors, the RK blends (the reference's
+// forms) and the stage-3 epilogue (CFL speed, div B, |B|, totals) are the FP64
+// kernel's arithmetic on the FP32 fluxes.
 #pragma once
 #include "stage_kernel.cuh"
 #include "tma.cuh"
@@ -53,6 +62,24 @@ template <int TX, int TY, bool SB> struct TileGeom32 : TileGeom<TX, TY> {
 template <int STAGE>
 __device__ __forceinline__ float rk_blend(float u0, float u) {
   return (STAGE == 2) ? u0 + 0.25f * (u - u0) : u0 + (2.0f / 3.0f) * (u - u0);
+}
+
+// A new face B of stage STAGE: b + dt * db (the curl of the FP32 corner Ez),
+// then the RK blend.  FP32 storage: FP32 arithmetic and the blend above; FP64
+// storage: FP64 arithmetic and the reference's blend forms
+// (src/main.f90:202-207, 261-266).
+template <int STAGE>
+__device__ __forceinline__ float blend_b(float b, float b0, float db, float dt, double) {
+  float val = b + dt * db;
+  if (STAGE >= 2) val = rk_blend<STAGE>(b0, val);
+  return val;
+}
+template <int STAGE>
+__device__ __forceinline__ double blend_b(double b, double b0, float db, float, double dt) {
+  double val = b + dt * double(db);
+  if (STAGE == 2) val = 0.75 * b0 + 0.25 * val;
+  if (STAGE == 3) val = (1.0 / 3.0) * b0 + (2.0 / 3.0) * val;
+  return val;
 }
 
 // The MC limiter (apply_slope_limiter, src/mhd_derivatives.f90:86-96) on a
@@ -151,10 +178,13 @@ __device__ __forceinline__ void tma_issue(const StageArgs& a, int w, float* stg,
   for (int q = 0; q < 6; ++q) tma_load_2d(stg + q * BOXF, maps + q * TMAP_BYTES, i0 - 4, j0 - 3, bar);
 }
 
-template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB, bool TMA>
+template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB, bool TMA, typename S = float>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   using G = TileGeom32<TX, TY, SB>;
   static_assert(!TMA || G::TMA_FITS, "TMA staging must fit in the slope arrays");
+  constexpr bool MIX = sizeof(S) == 8;   // FP64 storage, FP32 flux arithmetic
+  static_assert(!(TMA && MIX), "the TMA staging holds FP32 boxes");
+  static_assert(!MIX || 2 * (G::NBX + G::NBY) <= 12 * G::NS, "FP64 face-B arrays must fit in the slope arrays");
   using R = float;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);       // [6][NP]   primitives, tile + 2 halo
@@ -163,8 +193,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   R* sHi = sLo + 6 * G::NS;                     // [6][NS]   MOOD upper bounds (SB)
   R* sFx = sS + G::NSA * G::NS;                 // [5][NFX]
   R* sFy = sFx + 5 * G::NFX;                    // [5][NFY]
-  R* sBx = sS;                                  // new face B (phase 3a on): reuses the slopes
-  R* sBy = sBx + G::NBX;
+  S* sBx = reinterpret_cast<S*>(sS);            // new face B (phase 3a on): reuses the slopes
+  S* sBy = sBx + G::NBX;
   __shared__ double red[6 * (NT / 32)];
   __shared__ int s_last;
   __shared__ unsigned s_own;   // stage 3: bit r set if tile row r is one of the grid's own rows
@@ -204,7 +234,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       if (TMA && (s_tma & 1u)) {   // a copy was issued for this tile: consume it to keep the phases paired
         const bool ok = mbar_wait(&s_bar, (s_tma >> 1) & 1u, TMA_POLLS);
         if (__syncthreads_or(!ok)) {   // a copy that never lands sets the status word and ends the kernel
-          if (tid == 0) atomicOr(&ctl->status, STATUS_TIMEOUT);
+          if (tid == 0) {
+            atomicOr(&ctl->status, STATUS_TIMEOUT);
+            mbar_wait(&s_bar, (s_tma >> 1) & 1u, TMA_POLLS);   // a last bounded wait for the copy in flight
+          }
           return;
         }
         if (tid == 0) s_tma = (s_tma ^ 2u) & ~1u;
@@ -226,22 +259,26 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
     }
     const R gamma = R(g.gamma);
     const R vol = R(g.vol);
-    const R dt = R(ctl->dt);
+    const double dt64 = ctl->dt;
+    const R dt = R(dt64);
     const int sbuf = ctl->parity, obuf = 1 - sbuf;
     const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
     const int out_buf = (STAGE == 2) ? 2 : obuf;
-    const R* __restrict__ in[6];
-    const R* __restrict__ u0[6];
-    R* __restrict__ out[6];
+    // FP64 storage: set after phase 2 instead (see there)
+    const S* __restrict__ in[6];
+    const S* __restrict__ u0[6];
+    S* __restrict__ out[6];
+    if constexpr (!MIX) {
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
-      u0[q] = reinterpret_cast<const R*>(g.buf[sbuf][q]);
-      out[q] = reinterpret_cast<R*>(g.buf[out_buf][q]);
+      for (int q = 0; q < 6; ++q) {
+        in[q] = reinterpret_cast<const S*>(g.buf[in_buf][q]);
+        u0[q] = reinterpret_cast<const S*>(g.buf[sbuf][q]);
+        out[q] = reinterpret_cast<S*>(g.buf[out_buf][q]);
+      }
     }
     {
       const int wn = w + gridDim.x;   // the next tile's inputs are prefetched to L2 unless TMA loads them
-      prefetch_next_tile<R, TX, TY, NT, STAGE>(
+      prefetch_next_tile<S, TX, TY, NT, STAGE>(
           a, wn, !(TMA && wn < a.total_tiles && tma_tile<TX, TY, G::BW, G::BH>(a, wn)));
     }
 
@@ -267,10 +304,37 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         sP[4 * G::NP + p] = pr.Bx;
         sP[5 * G::NP + p] = pr.By;
       }
+    } else if constexpr (MIX) {
+      // FP64 storage: one element at a time, as the FP64 kernel (eight FP64
+      // loads per element in flight at once would spill); FP64 recovery
+      // (src/mhd_change_states.f90:61-113), rounded to FP32
+      const S* __restrict__ src[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) src[q] = reinterpret_cast<const S*>(g.buf[in_buf][q]);
+      for (int p = tid; p < G::NP; p += NT) {
+        const int qx = p % G::PX, qy = p / G::PX;
+        const int si = map_index(i0 - 2 + qx, nx, px);
+        const int sj = map_index(j0 - 2 + qy, ny, py);
+        const size_t idx = size_t(sj) * nx + si;
+        const double bxc = src[4][idx], byc = src[5][idx];
+        double Bx, By;
+        if (si > 0) Bx = 0.5 * (bxc + src[4][idx - 1]);
+        else Bx = px ? 0.5 * (bxc + src[4][idx + (nx - 1)]) : bxc;
+        if (sj > 0) By = 0.5 * (byc + src[5][idx - nx]);
+        else By = py ? 0.5 * (byc + src[5][idx + size_t(ny - 1) * nx]) : byc;
+        const Prim<double> pd = get_primitive<double>(src[0][idx], src[1][idx], src[2][idx], src[3][idx], Bx, By,
+                                                      g.gamma, g.vol);
+        sP[0 * G::NP + p] = float(pd.rho);
+        sP[1 * G::NP + p] = float(pd.vx);
+        sP[2 * G::NP + p] = float(pd.vy);
+        sP[3 * G::NP + p] = float(pd.P);
+        sP[4 * G::NP + p] = float(pd.Bx);
+        sP[5 * G::NP + p] = float(pd.By);
+      }
     } else {
       // all of this thread's loads are issued before any arithmetic (memory-level parallelism)
       constexpr int KP = (G::NP + NT - 1) / NT;
-      R ld[KP][8];
+      S ld[KP][8];
 #pragma unroll
       for (int k = 0; k < KP; ++k) {
         const int p = tid + k * NT;
@@ -292,14 +356,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
           const int qx = p % G::PX, qy = p / G::PX;
           const int si = map_index(i0 - 2 + qx, nx, px);
           const int sj = map_index(j0 - 2 + qy, ny, py);
-          const R Bx = (si > 0 || px) ? R(0.5) * (ld[k][4] + ld[k][5]) : ld[k][4];
-          const R By = (sj > 0 || py) ? R(0.5) * (ld[k][6] + ld[k][7]) : ld[k][6];
-          Prim<R> pr;
-          if constexpr (sizeof(R) == 4)
-            pr = get_primitive_mixed(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, g.gamma, g.inv_vol,
-                                     float(g.inv_vol));
-          else
-            pr = get_primitive<R>(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, gamma, vol);
+          const S Bx = (si > 0 || px) ? S(0.5) * (ld[k][4] + ld[k][5]) : ld[k][4];
+          const S By = (sj > 0 || py) ? S(0.5) * (ld[k][6] + ld[k][7]) : ld[k][6];
+          const Prim<R> pr = get_primitive_mixed(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, g.gamma,
+                                                 g.inv_vol, float(g.inv_vol));
           sP[0 * G::NP + p] = pr.rho;
           sP[1 * G::NP + p] = pr.vx;
           sP[2 * G::NP + p] = pr.vy;
@@ -311,7 +371,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
     }
     if constexpr (TMA) {
       if (__syncthreads_or(tma_bad)) {   // a copy that never lands sets the status word and ends the kernel
-        if (tid == 0) atomicOr(&ctl->status, STATUS_TIMEOUT);
+        if (tid == 0) {
+          atomicOr(&ctl->status, STATUS_TIMEOUT);
+          mbar_wait(&s_bar, (s_tma >> 1) & 1u, TMA_POLLS);   // a last bounded wait for the copy in flight
+        }
         return;
       }
     } else {
@@ -463,6 +526,17 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       }
     }
 
+    if constexpr (MIX) {
+      // the buffer pointers, read here rather than kept in registers through
+      // phases 1.5 and 2 (as the FP64 kernel does)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        in[q] = static_cast<const S*>(load_ptr(&g.buf[in_buf][q]));
+        u0[q] = static_cast<const S*>(load_ptr(&g.buf[sbuf][q]));
+        out[q] = static_cast<S*>(load_ptr(&g.buf[out_buf][q]));
+      }
+    }
+
     // ---- phase 3a: constrained transport -> new face B ----------------------------
     const R* FByX = sFx + 4 * G::NFX;
     const R* FBxY = sFy + 4 * G::NFY;
@@ -497,21 +571,19 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       const int gi = (i < 0) ? i + nx : i;
       const int gj = (j < 0) ? j + ny : j;
       const size_t idx = size_t(gj) * nx + gi;
-      R val;
+      S val;
       if (!isy) {
         const bool inner = j > 0 || py;
         const float2 e = Ez2(i, j, i, inner ? j - 1 : 1);
         const R dbx = inner ? ((-e.x) - (-e.y)) * inv_dy : ((-e.y) - (-e.x)) * inv_dy;   // outflow ylo: copy row 2
-        val = in[4][idx] + dt * dbx;
-        if (STAGE >= 2) val = rk_blend<STAGE>(u0[4][idx], val);
+        val = blend_b<STAGE>(in[4][idx], u0[4][idx], dbx, dt, dt64);
         if (STAGE == 3) sBx[lj * G::BXW + (li + 1)] = val;   // the epilogue reads neighbours' new B
         else out[4][idx] = val;                                // stages 1, 2: straight to the output
       } else {
         const bool inner = i > 0 || px;
         const float2 e = Ez2(i, j, inner ? i - 1 : 1, j);
         const R dby = inner ? -(((-e.x) - (-e.y)) * inv_dx) : -(((-e.y) - (-e.x)) * inv_dx);   // outflow xlo: copy column 2
-        val = in[5][idx] + dt * dby;
-        if (STAGE >= 2) val = rk_blend<STAGE>(u0[5][idx], val);
+        val = blend_b<STAGE>(in[5][idx], u0[5][idx], dby, dt, dt64);
         if (STAGE == 3) sBy[(lj + 1) * G::BYW + li] = val;
         else out[5][idx] = val;
       }
@@ -530,6 +602,80 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       const size_t idx = size_t(j) * nx + i;
       const int fxr = (lj + 1) * G::FXW + (li + 1);
       const int fyt = (lj + 1) * G::FYW + (li + 1);
+      if constexpr (MIX) {
+        // FP64 storage: the FP64 kernel's update on the FP32 fluxes --
+        // update_conserved (src/mhd_flux.f90:20-76), x pass then y pass,
+        // apply_conserved_floors with the stage's cell B, the outflow boundary
+        // correction (src/main.f90:118-148), the RK blend + floors
+        // (src/main.f90:202-208, 261-267)
+        const double ax64 = dt64 * g.dy, ay64 = dt64 * g.dx;
+        double U[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          double F = in[q][idx];
+          const R* fx = sFx + q * G::NFX;
+          const R* fy = sFy + q * G::NFY;
+          if (i > 0 || px) F = (F - ax64 * double(fx[fxr])) + ax64 * double(fx[fxr - 1]);
+          else F = F - ax64 * double(fx[fxr]);
+          if (j > 0 || py) F = (F - ay64 * double(fy[fyt])) + ay64 * double(fy[fyt - G::FYW]);
+          else F = F - ay64 * double(fy[fyt]);
+          U[q] = F;
+        }
+        const int pc = (lj + 2) * G::PX + (li + 2);
+        const double cr = sP[0 * G::NP + pc], cu = sP[1 * G::NP + pc], cv = sP[2 * G::NP + pc];
+        const double cP = sP[3 * G::NP + pc], cBx = sP[4 * G::NP + pc], cBy = sP[5 * G::NP + pc];
+        floor_hits += conserved_floors<double>(U[0], U[1], U[2], U[3], cBx, cBy, g.gamma, g.vol) ? 1u : 0u;
+        if (!px && i == 0) {
+          const double hb = 0.5 * (cBx * cBx + cBy * cBy);
+          const double en = ((cP - hb) / (g.gamma - 1.0) + 0.5 * cr * (cu * cu + cv * cv)) + hb;
+          U[0] = U[0] + ax64 * cr * cu;
+          U[1] = U[1] + ax64 * ((cr * (cu * cu) + cP) - cBx * cBx);
+          U[2] = U[2] + ax64 * (cr * cu * cv - cBx * cBy);
+          U[3] = U[3] + ax64 * ((en + cP) * cu - cBx * (cBx * cu + cBy * cv));
+        }
+        if (!py && j == 0) {
+          const double hb = 0.5 * (cBx * cBx + cBy * cBy);
+          const double en = ((cP - hb) / (g.gamma - 1.0) + 0.5 * cr * (cu * cu + cv * cv)) + hb;
+          U[0] = U[0] + ay64 * cr * cv;
+          U[2] = U[2] + ay64 * ((cr * (cv * cv) + cP) - cBy * cBy);
+          U[1] = U[1] + ay64 * (cr * cv * cu - cBy * cBx);
+          U[3] = U[3] + ay64 * ((en + cP) * cv - cBy * (cBy * cv + cBx * cu));
+        }
+        if (STAGE == 2) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) U[q] = 0.75 * u0[q][idx] + 0.25 * U[q];
+        }
+        if (STAGE == 3) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) U[q] = (1.0 / 3.0) * u0[q][idx] + (2.0 / 3.0) * U[q];
+        }
+        if (STAGE >= 2)
+          floor_hits += conserved_floors<double>(U[0], U[1], U[2], U[3], cBx, cBy, g.gamma, g.vol) ? 1u : 0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q][idx] = U[q];
+        if (STAGE == 3) {
+          const double bxn = sBx[lj * G::BXW + (li + 1)];
+          const double byn = sBy[(lj + 1) * G::BYW + li];
+          out[4][idx] = bxn;
+          out[5][idx] = byn;
+          if ((s_own >> lj) & 1u) {   // the FP64 epilogue (the CFL kernel's arithmetic)
+            const double bxm = sBx[lj * G::BXW + li];
+            const double bym = sBy[lj * G::BYW + li];
+            const bool hx = (i > 0) || px, hy = (j > 0) || py;
+            const double Bx = hx ? 0.5 * (bxn + bxm) : bxn;
+            const double By = hy ? 0.5 * (byn + bym) : byn;
+            const Prim<double> pr = get_primitive<double>(U[0], U[1], U[2], U[3], Bx, By, g.gamma, g.vol);
+            e_speed = run_max(e_speed, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
+            const double dv = fabs(divb_cell(bxn, bxm, byn, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
+            e_dmax = run_max(e_dmax, dv);
+            e_dsum += dv;
+            e_bmax = run_max(e_bmax, sqrt(Bx * Bx + By * By));
+            e_mass += U[0];
+            e_en += U[3];
+          }
+        }
+        continue;
+      } else {
       // update_conserved (src/mhd_flux.f90:20-76), x pass then y pass, fields
       // (0, 1) and (2, 3) as lanes of paired FP32 fused multiply-adds
       R U[4];
@@ -608,7 +754,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         e_mass += double(U[0]);
         e_en += double(U[3]);
       }
-    }
+          }
+}
     if (a.counters && !a.dry) {
       unsigned s = __reduce_add_sync(0xffffffffu, floor_hits);
       if ((tid & 31) == 0 && s) atomicAdd(&ctl->floor_hits, (unsigned long long)s);

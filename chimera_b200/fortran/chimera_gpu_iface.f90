@@ -11,7 +11,8 @@ module chimera_gpu_iface
     private
     public :: chimera_cfg, chimera_diag_out
     public :: chimera_create, chimera_destroy, chimera_set_state, chimera_get_state
-    public :: chimera_set_time, chimera_step, chimera_advance, chimera_diag, chimera_step_host
+    public :: chimera_set_time, chimera_step, chimera_advance, chimera_advance_output, chimera_diag
+    public :: chimera_step_host
     public :: chimera_batch_create, chimera_batch_set_state, chimera_batch_get_state
     public :: chimera_batch_set_time, chimera_batch_diag, chimera_set_graph_steps
     public :: chimera_autotune, chimera_set_variant
@@ -28,10 +29,10 @@ module chimera_gpu_iface
     public :: chimera_op_thermal_pressure_check, chimera_op_compute_fluxes
     public :: chimera_op_update_conserved, chimera_op_constrained_transport
     public :: chimera_op_compute_curl_2d, chimera_op_compute_divB
-    public :: CHIMERA_HOST, CHIMERA_DEVICE, CHIMERA_FP64, CHIMERA_FP32_BULK
+    public :: CHIMERA_HOST, CHIMERA_DEVICE, CHIMERA_FP64, CHIMERA_FP32_BULK, CHIMERA_FP32_MIXED
 
     integer(c_int), parameter :: CHIMERA_HOST = 0, CHIMERA_DEVICE = 1
-    integer(c_int), parameter :: CHIMERA_FP64 = 0, CHIMERA_FP32_BULK = 1
+    integer(c_int), parameter :: CHIMERA_FP64 = 0, CHIMERA_FP32_BULK = 1, CHIMERA_FP32_MIXED = 2
 
     type, bind(C) :: chimera_cfg
         integer(c_int)  :: nx, ny
@@ -101,6 +102,15 @@ module chimera_gpu_iface
         end function
 
         integer(c_int) function chimera_advance(h, max_steps, steps_taken) bind(C, name="chimera_advance")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            integer(c_int), value :: max_steps
+            integer(c_int), intent(out) :: steps_taken
+        end function
+
+        ! as chimera_advance, stopping after the step that reaches the next output time
+        integer(c_int) function chimera_advance_output(h, max_steps, steps_taken) &
+                bind(C, name="chimera_advance_output")
             import :: c_int, c_ptr
             type(c_ptr), value :: h
             integer(c_int), value :: max_steps

@@ -84,6 +84,7 @@ def lib():
         L.chimera_step.argtypes = [P, C.c_int]
         L.chimera_step_host.argtypes = [P, P * 6, P * 6, C.c_int]
         L.chimera_advance.argtypes = [P, C.c_int, C.POINTER(C.c_int)]
+        L.chimera_advance_output.argtypes = [P, C.c_int, C.POINTER(C.c_int)]
         L.chimera_stage.argtypes = [P, C.c_int, C.c_double]
         L.chimera_batch_diag.argtypes = [P, C.c_int, C.POINTER(CDiag)]
         L.chimera_set_counters.argtypes = [P, C.c_int]
@@ -253,6 +254,13 @@ class Solver:
     def advance(self, max_steps: int = 10 ** 9) -> int:
         n = C.c_int(0)
         _check(lib().chimera_advance(self._h, int(max_steps), C.byref(n)), "advance")
+        return n.value
+
+    def advance_output(self, max_steps: int = 10 ** 9) -> int:
+        """Run to the next output time (or t_end): stops after the step that
+        reaches it, where the reference writes a snapshot."""
+        n = C.c_int(0)
+        _check(lib().chimera_advance_output(self._h, int(max_steps), C.byref(n)), "advance_output")
         return n.value
 
     def stage(self, k: int, dt: float):

@@ -90,11 +90,14 @@ def run(cfg, state, precision: int = FP64, max_steps: int = 10 ** 7):
     try:
         s.set_state(state)
         dev = [torch.empty((cfg.ny, cfg.nx), dtype=torch.float64, device="cuda") for _ in range(6)]
-        oc = s.diag()["output_count"]
-        for _ in range(max_steps):
-            s.step(1)
+        d = s.diag()
+        oc, taken = d["output_count"], 0
+        while d["active"] and taken < max_steps:
+            # the time loop runs on the device up to the step that reaches the next
+            # output time (src/main.f90:279), where the reference writes a snapshot
+            taken += s.advance_output(max_steps - taken)
             d = s.diag()
-            if d["output_count"] != oc:          # this step reached an output time (src/main.f90:279)
+            if d["output_count"] != oc:
                 oc = d["output_count"]
                 s.get_state(out=dev)
                 Bx, By = ops.average_face_to_cell_B(c64, dev[4], dev[5])
@@ -102,8 +105,6 @@ def run(cfg, state, precision: int = FP64, max_steps: int = 10 ** 7):
                 p_th = Ptot - 0.5 * (Bx * Bx + By * By)
                 snaps.append(dict(t=d["t"], rho=rho.cpu().numpy(), Vx=vx.cpu().numpy(), Vy=vy.cpu().numpy(),
                                   P=p_th.cpu().numpy(), Bx=Bx.cpu().numpy(), By=By.cpu().numpy()))
-            if d["active"] == 0:
-                break
     finally:
         s.close()
     return snaps

@@ -47,7 +47,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from .config import BC_OUTFLOW, BC_PERIODIC, FP64, SolverConfig
+from .config import BC_OUTFLOW, BC_PERIODIC, FP32_BULK, SolverConfig
 
 GHOST = 7
 
@@ -122,7 +122,7 @@ class SlabSolver:
         self.solver = Solver([self.layout.cfg], stream=self.stream.cuda_stream)
         if self.layout.lo or self.layout.hi:
             self.solver.slab_ghost_rows(self.layout.lo, self.layout.hi)
-        store = torch.float64 if cfg.precision == FP64 else torch.float32
+        store = torch.float32 if cfg.precision == FP32_BULK else torch.float64
         shape = (6, ghost, cfg.nx)
         lo, hi = self.layout.lo, self.layout.hi
         self.send_lo = torch.empty(shape, dtype=store, device="cuda") if lo else None

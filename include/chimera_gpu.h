@@ -38,6 +38,9 @@ extern "C" {
 
 #define CHIMERA_FP64 0        /* plain FP64, bit-compatible with the reference expressions */
 #define CHIMERA_FP32_BULK 1   /* FP32 storage/arithmetic, FP64 pressure recovery, dt and sums */
+#define CHIMERA_FP32_MIXED 2  /* FP64 storage; FP32 reconstruction, limiter, MOOD and Riemann
+                                 arithmetic; FP64 pressure recovery, cell and face-B updates,
+                                 floors, RK blends, dt and sums */
 
 #define CHIMERA_HOST 0        /* pointer arguments are host memory */
 #define CHIMERA_DEVICE 1      /* pointer arguments are device memory */
@@ -66,7 +69,7 @@ typedef struct chimera_cfg {
   int limiter;             /* slope_limiter */
   int use_slope_limiting;  /* useSlopeLimiting */
   int mood;                /* fallback_2_MOOD */
-  int precision;           /* CHIMERA_FP64 or CHIMERA_FP32_BULK */
+  int precision;           /* CHIMERA_FP64, CHIMERA_FP32_BULK or CHIMERA_FP32_MIXED */
 } chimera_cfg;
 
 typedef struct chimera_diag_out {
@@ -129,6 +132,16 @@ int chimera_step(chimera_handle* h, int nsteps);
 /* Run until t >= t_end or max_steps steps (do while (t < tEnd),
  * src/main.f90:65); *steps_taken receives the count.  Synchronises. */
 int chimera_advance(chimera_handle* h, int max_steps, int* steps_taken);
+
+/* As chimera_advance, but every member also stops right after the step whose
+ * t reaches its next output time (t >= outputCount*tOut or t >= tEnd, the
+ * condition under which src/main.f90:279-292 writes a snapshot and advances
+ * outputCount): the time loop and its stop test stay on the device (graph
+ * replay, no host round trip per step), and the call returns with the state
+ * of the snapshot.  The snapshot cadence of the reference's loop is one call
+ * per output.  In a batch, members that stop early wait for the others.
+ * *steps_taken receives the largest step count of a member.  Synchronises. */
+int chimera_advance_output(chimera_handle* h, int max_steps, int* steps_taken);
 
 /* One RK stage k (1..3) with a given dt on the handle's stage buffers
  * (src/main.f90:107-149, 155-208, 214-267): stage 1 reads U^n, writes U1;
@@ -211,7 +224,8 @@ int chimera_get_variant(chimera_handle* h, int* variant, int* tile_x, int* tile_
  *   - pack:   lo <- state rows [rows, 2 rows), hi <- rows [ny - 2 rows, ny - rows)
  *   - unpack: state rows [0, rows) <- lo, rows [ny - rows, ny) <- hi
  * lo / hi are device buffers of 6 * rows * nx elements (field-major, Mass..b_y),
- * 8-byte elements for CHIMERA_FP64 and 4-byte ones for CHIMERA_FP32_BULK; a
+ * 8-byte elements for CHIMERA_FP64 and CHIMERA_FP32_MIXED, 4-byte ones for
+ * CHIMERA_FP32_BULK; a
  * null side is skipped.  Requires 2 * rows <= ny. */
 int chimera_halo_pack(chimera_handle* h, int rows, void* lo, void* hi);
 int chimera_halo_unpack(chimera_handle* h, int rows, const void* lo, const void* hi);

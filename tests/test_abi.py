@@ -377,7 +377,8 @@ def test_constants_agree_across_the_bindings():
         "CHIMERA_LIMITER_MC": config.MC, "CHIMERA_BC_PERIODIC": config.BC_PERIODIC,
         "CHIMERA_BC_FIXED": config.BC_FIXED, "CHIMERA_BC_OUTFLOW": config.BC_OUTFLOW,
         "CHIMERA_BC_INFLOW": config.BC_INFLOW, "CHIMERA_FP64": config.FP64,
-        "CHIMERA_FP32_BULK": config.FP32_BULK, "CHIMERA_HOST": gpu.HOST, "CHIMERA_DEVICE": gpu.DEVICE,
+        "CHIMERA_FP32_BULK": config.FP32_BULK, "CHIMERA_FP32_MIXED": config.FP32_MIXED,
+        "CHIMERA_HOST": gpu.HOST, "CHIMERA_DEVICE": gpu.DEVICE,
         "CHIMERA_OK": gpu.OK,
     }
     py.update({name: code for code, name in gpu.ERR.items()})

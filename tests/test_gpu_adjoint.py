@@ -13,7 +13,7 @@ import pytest
 import torch
 
 from chimera_b200 import problems as P
-from chimera_b200.config import HLLE, MC, RUSANOV, VAN_LEER
+from chimera_b200.config import FP32_BULK, FP32_MIXED, FP64, HLLE, MC, RUSANOV, VAN_LEER
 from tests.gpu_util import require_gpu
 
 pytestmark = pytest.mark.gpu
@@ -38,11 +38,11 @@ def _prims(cfg, st):
     return rho, vx, vy, p, bx, by
 
 
-def _loss_gpu(A, adj, cfg, prims, dts, K):
+def _loss_gpu(A, adj, cfg, prims, dts, K, precision=FP64):
     rho, vx, vy, p, bx, by = prims
     U0 = A.conserved_from_primitive(cfg, rho, vx, vy, p, bx, by)
     U0 = [u.contiguous() for u in U0]
-    UN = A.run(adj, U0, dts, K=K)
+    UN = A.run(adj, U0, dts, K=K, precision=precision)
     return A.magnetic_energy(cfg, UN)
 
 
@@ -111,13 +111,13 @@ def _smooth_dirs(shape, dx, dy, length, gen):
     return d / torch.max(torch.abs(d))
 
 
-def _fd_check(A, cfg, st, nsteps, ndirs, K, seed, eps_rel=1e-6, tol=1e-6, length=0.1):
+def _fd_check(A, cfg, st, nsteps, ndirs, K, seed, eps_rel=1e-6, tol=1e-6, length=0.1, precision=FP64):
     U0 = [torch.from_numpy(a.copy()).cuda() for a in st]
     dts = A.cfl_dts(cfg, U0, nsteps)
     prims = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in _prims(cfg, st)]
     adj = A.Adjoint(cfg)
     g_in = [x.clone().requires_grad_(k < 3) for k, x in enumerate(prims)]
-    loss = _loss_gpu(A, adj, cfg, g_in, dts, K)
+    loss = _loss_gpu(A, adj, cfg, g_in, dts, K, precision)
     loss.backward()
     grads = [g_in[k].grad for k in range(3)]
 
@@ -217,3 +217,67 @@ def test_adjoint_field_loop_512_400_steps(A):
     (measured), and the bound is 1e-2."""
     cfg, st = P.field_loop(512, 512, 2.0, 1.0, v=(2.0, 1.0), riemann=HLLE, limiter=VAN_LEER)
     _fd_check(A, cfg, st, nsteps=400, ndirs=16, K=20, seed=7, tol=1e-2, length=0.25)
+
+
+def _grads(A, cfg, st, nsteps, K, precision):
+    U0 = [torch.from_numpy(a.copy()).cuda() for a in st]
+    dts = A.cfl_dts(cfg, U0, nsteps)
+    prims = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in _prims(cfg, st)]
+    g_in = [x.clone().requires_grad_(k < 3) for k, x in enumerate(prims)]
+    loss = _loss_gpu(A, A.Adjoint(cfg), cfg, g_in, dts, K, precision)
+    loss.backward()
+    return loss.item(), [g_in[k].grad for k in range(3)]
+
+
+@pytest.mark.parametrize("precision", [FP32_BULK, FP32_MIXED])
+def test_adjoint_fp32_forward_generic_state(A, precision):
+    """The forward in FP32 (fused FP32 solver, same frozen dts; checkpoints
+    every K steps), the adjoint in FP64 from those checkpoints: on a generic
+    smooth state (HLLE + Van Leer, 40 steps, K = 10) the loss is the FP64
+    one to 1e-7 relative, the gradient the FP64-forward gradient to 5e-4 of
+    its scale (measured 1.2e-4), and FP64 central differences of the FP64
+    loss agree with it to 3e-5 (measured 6.5e-6; FP64 forward: 2e-8)."""
+    cfg, st = _generic_state(64, 21)
+    l64, g64 = _grads(A, cfg, st, 40, 10, FP64)
+    l32, g32 = _grads(A, cfg, st, 40, 10, precision)
+    assert abs(l32 - l64) <= 1e-7 * abs(l64)
+    for a, b in zip(g32, g64):
+        assert float(torch.max(torch.abs(a - b))) <= 5e-4 * float(torch.max(torch.abs(b)))
+    _fd_check(A, cfg, st, nsteps=40, ndirs=8, K=10, seed=1, eps_rel=1e-7, tol=3e-5, precision=precision)
+
+
+@pytest.mark.parametrize("precision", [FP32_BULK, FP32_MIXED])
+def test_adjoint_fp32_forward_field_loop_512(A, precision):
+    """The field-loop adjoint configuration with the FP32 forward and the FP64
+    check: 512^2 on [0,2]x[0,1], v = (2, 1), HLLE + Van Leer, 400 steps,
+    checkpoints every 20, FP64 central differences on 16 smooth random
+    directions.  As in the FP64-forward test the uniform rho and v put every
+    rho / v limiter at its kink, so central differences agree only to the
+    level the kinks allow; the FP32 trajectory's rounding moves some limiters
+    off their kinks, which the FP64 differences of the FP64 loss do not see
+    (measured worst of 16 directions: 1.7e-2 FP32-bulk, 1.1e-2 FP32-mixed,
+    against 2.7e-3 with the FP64 forward); the bound is 3e-2."""
+    cfg, st = P.field_loop(512, 512, 2.0, 1.0, v=(2.0, 1.0), riemann=HLLE, limiter=VAN_LEER)
+    _fd_check(A, cfg, st, nsteps=400, ndirs=16, K=20, seed=7, tol=3e-2, length=0.25, precision=precision)
+
+
+@pytest.mark.parametrize("precision", [FP32_BULK, FP32_MIXED])
+def test_adjoint_fp32_forward_vs_torch_autodiff(A, precision):
+    """The FP32-forward gradient against PyTorch FP64 autodiff of the
+    independent restatement at 64^2 (generic state, 15 steps): within 5e-4 of
+    the gradient scale (the FP64-forward gradient matches it to 1e-9)."""
+    from oracle import torch_ref as T
+    cfg, st = _generic_state(64, 5)
+    U0 = [torch.from_numpy(a.copy()).cuda() for a in st]
+    dts = A.cfl_dts(cfg, U0, 15)
+    prims = [torch.from_numpy(np.ascontiguousarray(x)) for x in _prims(cfg, st)]
+    g_in = [x.clone().cuda().requires_grad_(k < 3) for k, x in enumerate(prims)]
+    _loss_gpu(A, A.Adjoint(cfg), cfg, g_in, dts, 4, precision).backward()
+    c_in = [x.clone().requires_grad_(k < 3) for k, x in enumerate(prims)]
+    U = A.conserved_from_primitive(cfg, *c_in)
+    for dt in dts:
+        U = T.rk3_step(cfg, U, dt)
+    A.magnetic_energy(cfg, U).backward()
+    for k in range(3):
+        a, b = g_in[k].grad.cpu().numpy(), c_in[k].grad.numpy()
+        assert np.max(np.abs(a - b)) <= 5e-4 * np.max(np.abs(b))

@@ -142,6 +142,44 @@ def test_advance_to_t_end(G, oracle):
         assert np.array_equal(out[q], ref.a[q])
 
 
+@pytest.mark.parametrize("graph_steps", [0, 5])
+def test_advance_output_stops_at_every_output_time(G, oracle, graph_steps):
+    """chimera_advance_output: the device-resident loop stops right after each
+    step that reaches an output time (src/main.f90:279-292), with the oracle's
+    state, t and outputCount there, snapshot after snapshot, and with nothing
+    left paused after the last one (t_end)."""
+    cfg, st = P.orszag_tang(48, t_end=0.05)
+    cfg = cfg.replace(t_out=0.01)
+    ref = oracle.State(st)
+    s = G.Solver(cfg)
+    if graph_steps:
+        s.set_graph_steps(graph_steps)
+    s.set_state(st)
+    snaps = 0
+    while s.diag()["active"]:
+        oc0 = ref.output_count
+        n_ref = 0
+        while ref.output_count == oc0 and ref.t < cfg.t_end:   # the reference's loop to its next snapshot
+            n_ref += len(oracle.run(cfg, ref, 1))
+        n = s.advance_output()
+        d = s.diag()
+        assert n == n_ref and d["t"] == ref.t and d["output_count"] == ref.output_count
+        out = s.get_state()
+        for q in range(6):
+            assert np.array_equal(out[q], ref.a[q]), (snaps, q)
+        snaps += 1
+    assert snaps == 5 and d["t"] == ref.t and d["active"] == 0
+    assert s.advance_output() == 0            # t >= t_end: nothing more to do
+    # a member resumed after its pause steps on with chimera_step
+    s.set_time(0.0, 1)
+    s.set_state(st)
+    s.advance_output()
+    t1 = s.diag()["t"]
+    s.step(1)
+    d = s.diag()
+    assert d["t"] > t1 and d["active"] == 1 and d["output_count"] == 2
+
+
 def test_graph_replay_matches_eager(G):
     cfg, st = P.rotor(64)
     a = G.Solver(cfg)
@@ -239,8 +277,21 @@ def test_every_tile_variant_bitwise(G, oracle, solver):
         s.set_variant(v)
         s.step(8)
         out = s.get_state()
-        for q in range(6):
-            assert np.array_equal(out[q], ref.a[q]), (v, s.variant(), q)
+        bad = [q for q in range(6) if not np.array_equal(out[q], ref.a[q])]
+        if bad:
+            # report the size of the difference and whether a fresh handle
+            # reproduces it, then fail
+            q = bad[0]
+            t = G.Solver(cfg)
+            t.set_variant(v)
+            t.set_state(st)
+            t.step(8)
+            again = t.get_state()
+            t.close()
+            fresh_ok = all(np.array_equal(again[k], ref.a[k]) for k in range(6))
+            pytest.fail(f"variant {v} {s.variant()}: fields {bad} differ from the oracle, field {q}: "
+                        f"{int(np.sum(out[q] != ref.a[q]))} cells, max {max_ulp(out[q], ref.a[q])} ulp; "
+                        f"a fresh handle of this variant matches the oracle: {fresh_ok}")
 
 
 def test_autotune_keeps_state(G, oracle):
