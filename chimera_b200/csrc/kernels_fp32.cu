@@ -8,7 +8,8 @@ namespace chimera {
 
 namespace {
 // Storage type ST: float (FP32-bulk) or double (FP32 arithmetic on FP64
-// storage, whose dt comes from the FP64 CFL kernel, as its epilogue's does).
+// storage, whose CFL kernel has the FP64 epilogue's arithmetic; compiled in this
+// unit, its own instantiation).
 template <int TX, int TY, int NT, int MINB, bool SB = true, bool TMA = false, typename ST = float>
 void fill(KernelSet* ks) {
   using G = TileGeom32<TX, TY, SB>;
@@ -21,7 +22,7 @@ void fill(KernelSet* ks) {
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
 #undef CHIMERA_ENTRY
-  ks->cfl = KernelEntry{(const void*)&cfl_kernel<ST, TX, TY, NT>, 0, TX, TY, NT};
+  ks->cfl = KernelEntry{(const void*)&cfl_kernel<ST, TX, TY, NT, UNIT_FP32>, 0, TX, TY, NT};
   ks->elem_bytes = int(sizeof(ST));
 }
 }  // namespace

@@ -19,7 +19,7 @@ void fill(KernelSet* ks) {
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
 #undef CHIMERA_ENTRY
-  ks->cfl = KernelEntry{(const void*)&cfl_kernel<double, TX, TY, NT>, 0, TX, TY, NT};
+  ks->cfl = KernelEntry{(const void*)&cfl_kernel<double, TX, TY, NT, UNIT_FP64>, 0, TX, TY, NT};
   ks->elem_bytes = 8;
 }
 }  // namespace

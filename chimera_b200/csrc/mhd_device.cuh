@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace chimera {
 
 // src/mhd_config.f90:27-43
@@ -56,6 +58,15 @@ __device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
 __device__ __forceinline__ double dcopysign(double a, double b) { return copysign(a, b); }
 __device__ __forceinline__ float dcopysign(float a, float b) { return copysignf(a, b); }
 __device__ __forceinline__ bool disfinite(double a) { return isfinite(a); }
+
+// sqrt(0.5 (q + |q|)) for q > 0 or NaN: there 0.5 (q + |q|) = 0.5 (2 q) = q
+// exactly (both products by powers of two), so plain float / double take
+// sqrt(q); other arithmetic types (the adjoint's dual numbers) keep the
+// reference's expression (src/mhd_flux.f90:277-278, 355-358).
+template <typename R> __device__ __forceinline__ R sqrt_pos_part(R q) {
+  if constexpr (std::is_floating_point<R>::value) return dsqrt(q);
+  else return dsqrt(R(0.5) * (q + habs(q)));
+}
 __device__ __forceinline__ bool disfinite(float a) { return isfinite(a); }
 
 // A running maximum: max(run, x) as fmax(run, x) gives it for a run that is
@@ -128,7 +139,14 @@ __device__ __forceinline__ R limit_slope(R dfL, R dfR) {
   if (prod <= R(0) || habs(den) < R(1e-12)) return R(0);
   if (LIMITER == LIMITER_VAN_LEER) return (R(2) * prod) / den;
   // here dfL and dfR are nonzero with one sign and |den| >= 1e-12
-  return dcopysign(R(1), dfL) * hmin(hmin(R(2) * habs(dfL), R(2) * habs(dfR)), R(0.5) * habs(den));
+  if constexpr (std::is_floating_point<R>::value) {
+    // The same value with fewer operations: min(2|a|, 2|b|) = 2 min(|a|, |b|)
+    // (a product by 2 is exact), and sign(1, a) * m = copysign(m, a) for the
+    // non-negative m (a product by +-1 is exact).
+    return dcopysign(hmin(R(2) * hmin(habs(dfL), habs(dfR)), R(0.5) * habs(den)), dfL);
+  } else {   // other arithmetic types (the adjoint's dual numbers): the reference's form
+    return dcopysign(R(1), dfL) * hmin(hmin(R(2) * habs(dfL), R(2) * habs(dfR)), R(0.5) * habs(den));
+  }
 }
 
 // One face's 5 fluxes in (normal, tangential) orientation.
@@ -164,9 +182,9 @@ __device__ __forceinline__ Flux5<R> rusanov(R gamma, R rho_L, R rho_R, R vx_L, R
   F.bt = (By_avg * momx_avg - Bx_avg * momy_avg) * inv_rho_avg;
   R c_L2 = (gamma * p_th_L + R(2) * halfBL2) / rho_L;
   R c_R2 = (gamma * p_th_R + R(2) * halfBR2) / rho_R;
-  // c_L2, c_R2 > 0 (the thermal pressure is floored), so C_L, C_R > 0
-  R C_L = dsqrt(R(0.5) * (c_L2 + habs(c_L2))) + habs(vx_L);
-  R C_R = dsqrt(R(0.5) * (c_R2 + habs(c_R2))) + habs(vx_R);
+  // c_L2, c_R2 > 0 (the thermal pressure is floored; a NaN P floors to it), so C_L, C_R > 0
+  R C_L = sqrt_pos_part(c_L2) + habs(vx_L);
+  R C_R = sqrt_pos_part(c_R2) + habs(vx_R);
   R C = R(0.5) * hmax(C_L, C_R);
   F.mass = F.mass - C * (rho_R - rho_L);
   F.momn = F.momn - C * (rho_R * vx_R - rho_L * vx_L);
@@ -190,8 +208,8 @@ __device__ __forceinline__ Flux5<R> hlle(R gamma, R rho_L, R rho_R, R vx_L, R vx
   R en_R = (p_th_R / gm1 + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
   R qL = (gamma * p_th_L + R(2) * halfBL2) / rho_L;
   R qR = (gamma * p_th_R + R(2) * halfBR2) / rho_R;
-  R c_fL = hmin(dsqrt(R(0.5) * (qL + habs(qL))), cf_max_hlle);   // qL, qR > 0
-  R c_fR = hmin(dsqrt(R(0.5) * (qR + habs(qR))), cf_max_hlle);
+  R c_fL = hmin(sqrt_pos_part(qL), cf_max_hlle);   // qL, qR > 0 (or NaN)
+  R c_fR = hmin(sqrt_pos_part(qR), cf_max_hlle);
   R S_L = dmin(vx_L - c_fL, vx_R - c_fR);
   R S_R = dmax(vx_L + c_fL, vx_R + c_fR);
   R FL_Mass = rho_L * vx_L;

@@ -179,22 +179,22 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   k_noalloc_init<<<1, 32, 0, s>>>(d_member, d_ctl, g, *t, *output_count);
   const int grid = a.total_tiles;
   const size_t smem = TileGeom<NA_TX, NA_TY>::smem_bytes<double>();
-  cfl_kernel<double, NA_TX, NA_TY, NA_NT><<<grid, NA_NT, 0, s>>>(a);
+  cfl_kernel<double, NA_TX, NA_TY, NA_NT, UNIT_NOALLOC><<<grid, NA_NT, 0, s>>>(a);
   switch (cfg->riemann) {
     case CHIMERA_RIEMANN_RUSANOV:
-      stage_kernel<double, 1, 1, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
-      stage_kernel<double, 1, 2, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
-      stage_kernel<double, 1, 3, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 1, 1, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 1, 2, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 1, 3, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
       break;
     case CHIMERA_RIEMANN_HLLE:
-      stage_kernel<double, 2, 1, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
-      stage_kernel<double, 2, 2, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
-      stage_kernel<double, 2, 3, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 2, 1, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 2, 2, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 2, 3, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
       break;
     default:
-      stage_kernel<double, 3, 1, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
-      stage_kernel<double, 3, 2, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
-      stage_kernel<double, 3, 3, NA_TX, NA_TY, NA_NT, NA_MINB><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 3, 1, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 3, 2, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
+      stage_kernel<double, 3, 3, NA_TX, NA_TY, NA_NT, NA_MINB, false, false, UNIT_NOALLOC><<<grid, NA_NT, smem, s>>>(a);
       break;
   }
   if (cudaGetLastError() != cudaSuccess) return fail();

@@ -28,6 +28,15 @@ namespace chimera {
 
 // Work-list / member descriptors (device side), see chimera_types.h.
 
+// The translation unit that instantiates a kernel template, a template
+// argument of the stage and CFL kernels.  Units are compiled with different
+// floating-point flags (the FP64 units without multiply-add contraction, the
+// FP32 unit with fast math), and one template instantiation -- one kernel
+// symbol -- compiled in two units would give two device bodies under one name,
+// of which a launch runs whichever module the runtime resolved the name to.
+// Each unit passes its own value, so every instantiation is defined once.
+enum { UNIT_FP64 = 0, UNIT_FP32 = 1, UNIT_NOALLOC = 2 };
+
 // A pointer read from global memory where it is used (inline PTX, so that the
 // compiler neither hoists the read nor merges it with an earlier one): keeps
 // the value out of registers through a phase that needs them all.  Only for
@@ -285,7 +294,7 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
 // 32 x 16 tile; fewer live registers through the update, and fewer spills).
 // ----------------------------------------------------------------------------
 template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool KEEP_IN = false,
-          bool TMA = false>
+          bool TMA = false, int UNIT = UNIT_FP64>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   using G = TileGeom<TX, TY>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -705,8 +714,9 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
 // ----------------------------------------------------------------------------
 // CFL kernel: dt of the current state (src/main.f90:69-83) without advancing
 // time; used before the first step after the state is set.
+// UNIT: the translation unit that instantiates it (see UNIT_FP64).
 // ----------------------------------------------------------------------------
-template <typename R, int TX, int TY, int NT>
+template <typename R, int TX, int TY, int NT, int UNIT>
 __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
   __shared__ double red[6 * (NT / 32)];
   __shared__ int s_last;
