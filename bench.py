@@ -307,8 +307,9 @@ def cpu_reference_rate(n, repeats=3, seconds=10.0, omp_mode=2):
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    # --steps sets the number of timed samples (at least 3, each >= 10 s of CPU work)
-    r = cpu_reference_rate(args.n, repeats=max(3, min(args.steps, 5)), seconds=args.ref_seconds)
+    # three timed samples of >= 10 s each, as cpu_baseline takes them: the host's all-core
+    # clock settles over the first minute of load, so both take the same number
+    r = cpu_reference_rate(args.n, repeats=3, seconds=args.ref_seconds)
     rate = r["value"]
     line = {
         "impl": "reference",

@@ -828,10 +828,14 @@ int chimera_advance(chimera_handle* h, int max_steps, int* steps_taken) {
   std::vector<unsigned long long> s0(h->n);
   CK(cudaMemcpyAsync(c.data(), h->d_ctl, sizeof(Control) * h->n, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int m = 0; m < h->n; ++m) s0[m] = c[m].steps;
+  bool any_active = false;
+  for (int m = 0; m < h->n; ++m) {
+    s0[m] = c[m].steps;
+    any_active = any_active || c[m].active;
+  }
   int done = 0;
   const int chunk = 16;
-  while (done < max_steps) {
+  while (any_active && done < max_steps) {
     const int k = std::min(chunk, max_steps - done);
     int rc = run_steps(h, k);
     if (rc) return rc;

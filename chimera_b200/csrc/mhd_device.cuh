@@ -256,12 +256,35 @@ __device__ __forceinline__ Flux5<R> hll_avg(R SL, R SR, const Flux5<R>& FL, cons
   return F;
 }
 
+// The catch-all guard of hlld_flux (src/mhd_flux.f90:747-768): a flux that is
+// not finite or exceeds FAC_BND times a bound built from the two physical
+// fluxes and states is replaced by the HLL average.
+template <typename R>
+__device__ __forceinline__ Flux5<R> hlld_guard(Flux5<R> F, R SL, R SR, const Flux5<R>& FL, const Flux5<R>& FR, R rhoL,
+                                               R rhoR, R vxL, R vxR, R vyL, R vyR, R enL, R enR, R ByL, R ByR, R dM,
+                                               R dMn, R dMt, R dE, R dB) {
+  const R FAC_BND = R(8.0);
+  R Smax = hmax(habs(SL), habs(SR));
+  R bnd_mass = hmax(habs(FL.mass), habs(FR.mass)) + Smax * (rhoL + rhoR);
+  R bnd_momx = hmax(habs(FL.momn), habs(FR.momn)) + Smax * (habs(rhoL * vxL) + habs(rhoR * vxR));
+  R bnd_momy = hmax(habs(FL.momt), habs(FR.momt)) + Smax * (habs(rhoL * vyL) + habs(rhoR * vyR));
+  R bnd_enr = hmax(habs(FL.energy), habs(FR.energy)) + Smax * (habs(enL) + habs(enR));
+  R bnd_by = hmax(habs(FL.bt), habs(FR.bt)) + Smax * (habs(ByL) + habs(ByR));
+  bool use_hll = false;
+  if (!disfinite(F.mass) || habs(F.mass) > FAC_BND * bnd_mass) use_hll = true;
+  if (!disfinite(F.momn) || habs(F.momn) > FAC_BND * bnd_momx) use_hll = true;
+  if (!disfinite(F.momt) || habs(F.momt) > FAC_BND * bnd_momy) use_hll = true;
+  if (!disfinite(F.energy) || habs(F.energy) > FAC_BND * bnd_enr) use_hll = true;
+  if (!disfinite(F.bt) || habs(F.bt) > FAC_BND * bnd_by) use_hll = true;
+  if (use_hll) F = hll_avg(SL, SR, FL, FR, dM, dMn, dMt, dE, dB);
+  return F;
+}
+
 // src/mhd_flux.f90:408-779 (hlld_flux), one interface.
 template <typename R>
 __device__ __forceinline__ Flux5<R> hlld(R gamma, R rhoL, R rhoR, R vxL, R vxR, R vyL, R vyR,
                                          R pTL, R pTR, R BxL, R BxR, R ByL, R ByR) {
   const R EPS_FAN = R(1.0e-6);
-  const R FAC_BND = R(8.0);
   const R cf_max_hlld = R(50.0);
   R halfBL2 = R(0.5) * (BxL * BxL + ByL * ByL);
   R halfBR2 = R(0.5) * (BxR * BxR + ByR * ByR);
@@ -388,21 +411,7 @@ __device__ __forceinline__ Flux5<R> hlld(R gamma, R rhoL, R rhoR, R vxL, R vxR, 
     }
   }
 
-  // catch-all guard :747-768
-  R Smax = hmax(habs(SL), habs(SR));
-  R bnd_mass = hmax(habs(FL.mass), habs(FR.mass)) + Smax * (rhoL + rhoR);
-  R bnd_momx = hmax(habs(FL.momn), habs(FR.momn)) + Smax * (habs(rhoL * vxL) + habs(rhoR * vxR));
-  R bnd_momy = hmax(habs(FL.momt), habs(FR.momt)) + Smax * (habs(rhoL * vyL) + habs(rhoR * vyR));
-  R bnd_enr = hmax(habs(FL.energy), habs(FR.energy)) + Smax * (habs(enL) + habs(enR));
-  R bnd_by = hmax(habs(FL.bt), habs(FR.bt)) + Smax * (habs(ByL) + habs(ByR));
-  bool use_hll = false;
-  if (!disfinite(F.mass) || habs(F.mass) > FAC_BND * bnd_mass) use_hll = true;
-  if (!disfinite(F.momn) || habs(F.momn) > FAC_BND * bnd_momx) use_hll = true;
-  if (!disfinite(F.momt) || habs(F.momt) > FAC_BND * bnd_momy) use_hll = true;
-  if (!disfinite(F.energy) || habs(F.energy) > FAC_BND * bnd_enr) use_hll = true;
-  if (!disfinite(F.bt) || habs(F.bt) > FAC_BND * bnd_by) use_hll = true;
-  if (use_hll) F = hll_avg(SL, SR, FL, FR, dM, dMn, dMt, dE, dB);
-  return F;
+  return hlld_guard(F, SL, SR, FL, FR, rhoL, rhoR, vxL, vxR, vyL, vyR, enL, enR, ByL, ByR, dM, dMn, dMt, dE, dB);
 }
 
 template <typename R, int SOLVER>
