@@ -294,6 +294,27 @@ def test_every_tile_variant_bitwise(G, oracle, solver):
                         f"a fresh handle of this variant matches the oracle: {fresh_ok}")
 
 
+def test_tma_and_plain_loads_in_one_batch(G, oracle):
+    """The default variant loads interior tiles by TMA where the member has
+    tensor maps; a member whose row pitch is not a multiple of 16 bytes (odd
+    nx) has none and takes the plain loads everywhere.  A batch holding both,
+    and the odd grid alone, match the oracle bit for bit."""
+    members = [P.orszag_tang(96, riemann=HLLE), P.field_loop(101, 64, 101.0 / 64.0, 1.0, riemann=HLLE, limiter=MC)]
+    cfgs = [c for c, _ in members]
+    s = G.Solver(cfgs)
+    s.set_variant(0)
+    for m, (_, st) in enumerate(members):
+        s.set_state(st, member=m)
+    s.step(6)
+    for m, (cfg, st) in enumerate(members):
+        ref = oracle.State(st)
+        oracle.run(cfg, ref, 6)
+        out = s.get_state(member=m)
+        for q in range(6):
+            assert np.array_equal(out[q], ref.a[q]), (m, q)
+    s.close()
+
+
 def test_autotune_keeps_state(G, oracle):
     """Autotuning runs dry steps only: state and time-loop counters unchanged."""
     cfg, st = P.rotor(128)
