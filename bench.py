@@ -59,6 +59,8 @@ def parse():
                    help="also measure the Kelvin-Helmholtz HLLD comparison (FP32-bulk vs FP64)")
     p.add_argument("--kh-n", type=int, default=4096)
     p.add_argument("--kh-steps", type=int, default=1000)
+    p.add_argument("--kh-variant", type=int, default=-1,
+                   help="force a tile variant for the FP64 form of the Kelvin-Helmholtz leg (-1: autotune)")
     p.add_argument("--adjoint", choices=("on", "off"), default="on",
                    help="also measure the field-loop adjoint (forward + backward, central differences)")
     p.add_argument("--adj-steps", type=int, default=400, help="RK3 steps of the field-loop adjoint leg")
@@ -622,7 +624,10 @@ def run_kh(args):
     for name, prec in (("fp32_bulk", FP32_BULK), ("fp32_mixed", FP32_MIXED), ("fp64", FP64)):
         s = gpu.Solver(cfg.replace(precision=prec))
         s.set_state(st)
-        s.autotune(reps=1)
+        if prec == FP64 and args.kh_variant >= 0:
+            s.set_variant(args.kh_variant)
+        else:
+            s.autotune(reps=1)
         s.set_graph_steps(graph)
         s.step(graph)                                   # capture (not timed)
         s.set_state(st)

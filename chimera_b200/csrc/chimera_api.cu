@@ -489,6 +489,8 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
     g.vol = c.dx * c.dy;
     g.len = (c.dx < c.dy) ? c.dx : c.dy;
     g.inv_vol = 1.0 / g.vol;
+    g.rcp_vol = shared_reciprocal(g.vol);
+    g.rcp_gm1 = shared_reciprocal(c.gamma - 1.0);
     g.courant = c.courant;
     g.t_out = c.t_out;
     g.t_end = c.t_end;

@@ -35,6 +35,8 @@ struct Member {
   double hx, hy;           // 0.5*dx, 0.5*dy
   double gamma, vol, len;  // vol = dx*dy, len = min(dx, dy)
   double inv_vol;          // 1/vol (FP32-bulk pressure recovery)
+  double rcp_vol, rcp_gm1; // RN(1/vol), RN(1/(gamma - 1)) for the reciprocal divisions (div_by),
+                           // or 0 for a divisor outside 2^-120 <= b < 2^121 (shared_reciprocal)
   double courant, t_out, t_end;
   int skip_lo, skip_hi;     // rows at the bottom / top that the CFL kernel's dt and diagnostics
                            // leave out (the ghost rows of a y-slab; 0 otherwise)
@@ -42,6 +44,14 @@ struct Member {
   const void* tmap;        // TMA variants: this member's tensor maps [buffer 3][field 6] (CUtensorMap,
                            // 128 bytes each, boxes of the variant's tile) in device memory, or null
 };
+
+// RN(1/b) for a divisor b fixed for the launch, or 0 (IEEE division throughout)
+// where b lies outside 2^-120 <= |b| < 2^121, the range the reciprocal
+// division (div_by in mhd_device.cuh) is exact for.
+inline double shared_reciprocal(double b) {
+  const double m = b < 0 ? -b : b;
+  return (m >= 0x1p-120 && m < 0x1p121) ? 1.0 / b : 0.0;
+}
 
 // Time-loop state of one member, resident on the device so that whole runs
 // can be captured in a CUDA graph.

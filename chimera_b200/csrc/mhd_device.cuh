@@ -69,6 +69,27 @@ template <typename R> __device__ __forceinline__ R sqrt_pos_part(R q) {
 }
 __device__ __forceinline__ bool disfinite(float a) { return isfinite(a); }
 
+// a / b through a reciprocal y = RN(1/b) fixed for the launch (the cell volume,
+// gamma - 1): q = RN(a y), r = fma(-q, b, a), RN(q + r y) -- one correction
+// step (P. Markstein, IBM J. Res. Dev. 34(1), 1990) -- is the correctly rounded
+// quotient RN(a / b) when no step underflows or overflows.  The host gives
+// y = 0 for a b outside 2^-120 <= |b| < 2^121; a numerator outside
+// 2^-900 <= |a| < 2^900 (zero, subnormal, huge, Inf, NaN) takes IEEE division.
+// In that range q and r y stay normal and r = a - q b is exact.
+// tests/numerics/div_sweep.c compares it with IEEE division on random
+// quotients and on quotients within a few 2^-106 of a rounding midpoint.
+// Other arithmetic types divide.
+template <typename R> __device__ __forceinline__ R div_by(R a, R b, double) { return a / b; }
+template <> __device__ __forceinline__ double div_by<double>(double a, double b, double y) {
+  const unsigned e = (unsigned(__double2hiint(a)) >> 20) & 0x7ffu;   // biased exponent of a
+  if (y != 0.0 && e - 123u < 1800u) {
+    const double q = a * y;
+    const double r = fma(-q, b, a);
+    return fma(r, y, q);
+  }
+  return a / b;
+}
+
 // A running maximum: max(run, x) as fmax(run, x) gives it for a run that is
 // not NaN (a NaN x leaves run), as one compare and select -- FP64 fmax takes
 // several instructions on sm_100.
@@ -80,14 +101,16 @@ template <typename R> struct Prim {
 };
 
 // src/mhd_change_states.f90:61-113 (get_primitive), one cell.
+// rcp_vol: RN(1/vol) for div_by, or 0.
 template <typename R>
-__device__ __forceinline__ Prim<R> get_primitive(R M, R Mx, R My, R E, R Bx, R By, R gamma, R vol) {
+__device__ __forceinline__ Prim<R> get_primitive(R M, R Mx, R My, R E, R Bx, R By, R gamma, R vol,
+                                                 double rcp_vol = 0.0) {
   Prim<R> p;
-  R r = hmax(M / vol, K<R>::rho_floor);
+  R r = hmax(div_by(M, vol, rcp_vol), K<R>::rho_floor);
   R u = Mx / (r * vol);
   R v = My / (r * vol);
   R halfB2 = R(0.5) * (Bx * Bx + By * By);
-  R P = ((E / vol - R(0.5) * r * (u * u + v * v)) - halfB2) * (gamma - R(1)) + halfB2;
+  R P = ((div_by(E, vol, rcp_vol) - R(0.5) * r * (u * u + v * v)) - halfB2) * (gamma - R(1)) + halfB2;
   P = hmax(P, K<R>::P_floor);
   P = hmax(P, halfB2 + K<R>::e_floor_frac * (R(0.5) * r * (u * u + v * v) + halfB2));
   p.rho = r; p.vx = u; p.vy = v; p.P = P; p.Bx = Bx; p.By = By;
@@ -157,15 +180,16 @@ template <typename R> struct Flux5 {
 // src/mhd_flux.f90:197-288 (rusanov_flux), one interface.
 template <typename R>
 __device__ __forceinline__ Flux5<R> rusanov(R gamma, R rho_L, R rho_R, R vx_L, R vx_R, R vy_L, R vy_R,
-                                            R P_L, R P_R, R Bx_L, R Bx_R, R By_L, R By_R) {
+                                            R P_L, R P_R, R Bx_L, R Bx_R, R By_L, R By_R,
+                                            double rcp_gm1 = 0.0) {
   Flux5<R> F;
   R halfBL2 = R(0.5) * (Bx_L * Bx_L + By_L * By_L);
   R halfBR2 = R(0.5) * (Bx_R * Bx_R + By_R * By_R);
   R p_th_L = hmax(P_L - halfBL2, K<R>::P_floor);
   R p_th_R = hmax(P_R - halfBR2, K<R>::P_floor);
   R gm1 = gamma - R(1);
-  R en_L = (p_th_L / gm1 + R(0.5) * rho_L * (vx_L * vx_L + vy_L * vy_L)) + halfBL2;
-  R en_R = (p_th_R / gm1 + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
+  R en_L = (div_by(p_th_L, gm1, rcp_gm1) + R(0.5) * rho_L * (vx_L * vx_L + vy_L * vy_L)) + halfBL2;
+  R en_R = (div_by(p_th_R, gm1, rcp_gm1) + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
   R rho_avg = R(0.5) * (rho_L + rho_R);
   R inv_rho_avg = R(1) / rho_avg;
   R momx_avg = R(0.5) * (rho_L * vx_L + rho_R * vx_R);
@@ -197,15 +221,16 @@ __device__ __forceinline__ Flux5<R> rusanov(R gamma, R rho_L, R rho_R, R vx_L, R
 // src/mhd_flux.f90:291-405 (hlle_flux), one interface.
 template <typename R>
 __device__ __forceinline__ Flux5<R> hlle(R gamma, R rho_L, R rho_R, R vx_L, R vx_R, R vy_L, R vy_R,
-                                         R P_L, R P_R, R Bx_L, R Bx_R, R By_L, R By_R) {
+                                         R P_L, R P_R, R Bx_L, R Bx_R, R By_L, R By_R,
+                                         double rcp_gm1 = 0.0) {
   const R cf_max_hlle = R(1.0e2);
   R halfBL2 = R(0.5) * (Bx_L * Bx_L + By_L * By_L);
   R halfBR2 = R(0.5) * (Bx_R * Bx_R + By_R * By_R);
   R p_th_L = hmax(P_L - halfBL2, K<R>::P_floor);
   R p_th_R = hmax(P_R - halfBR2, K<R>::P_floor);
   R gm1 = gamma - R(1);
-  R en_L = (p_th_L / gm1 + R(0.5) * rho_L * (vx_L * vx_L + vy_L * vy_L)) + halfBL2;
-  R en_R = (p_th_R / gm1 + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
+  R en_L = (div_by(p_th_L, gm1, rcp_gm1) + R(0.5) * rho_L * (vx_L * vx_L + vy_L * vy_L)) + halfBL2;
+  R en_R = (div_by(p_th_R, gm1, rcp_gm1) + R(0.5) * rho_R * (vx_R * vx_R + vy_R * vy_R)) + halfBR2;
   R qL = (gamma * p_th_L + R(2) * halfBL2) / rho_L;
   R qR = (gamma * p_th_R + R(2) * halfBR2) / rho_R;
   R c_fL = hmin(sqrt_pos_part(qL), cf_max_hlle);   // qL, qR > 0 (or NaN)
@@ -283,7 +308,7 @@ __device__ __forceinline__ Flux5<R> hlld_guard(Flux5<R> F, R SL, R SR, const Flu
 // src/mhd_flux.f90:408-779 (hlld_flux), one interface.
 template <typename R>
 __device__ __forceinline__ Flux5<R> hlld(R gamma, R rhoL, R rhoR, R vxL, R vxR, R vyL, R vyR,
-                                         R pTL, R pTR, R BxL, R BxR, R ByL, R ByR) {
+                                         R pTL, R pTR, R BxL, R BxR, R ByL, R ByR, double rcp_gm1 = 0.0) {
   const R EPS_FAN = R(1.0e-6);
   const R cf_max_hlld = R(50.0);
   R halfBL2 = R(0.5) * (BxL * BxL + ByL * ByL);
@@ -291,8 +316,8 @@ __device__ __forceinline__ Flux5<R> hlld(R gamma, R rhoL, R rhoR, R vxL, R vxR, 
   R p_thL = hmax(pTL - halfBL2, K<R>::P_floor);
   R p_thR = hmax(pTR - halfBR2, K<R>::P_floor);
   R gm1 = gamma - R(1);
-  R enL = (p_thL / gm1 + R(0.5) * rhoL * (vxL * vxL + vyL * vyL)) + halfBL2;
-  R enR = (p_thR / gm1 + R(0.5) * rhoR * (vxR * vxR + vyR * vyR)) + halfBR2;
+  R enL = (div_by(p_thL, gm1, rcp_gm1) + R(0.5) * rhoL * (vxL * vxL + vyL * vyL)) + halfBL2;
+  R enR = (div_by(p_thR, gm1, rcp_gm1) + R(0.5) * rhoR * (vxR * vxR + vyR * vyR)) + halfBR2;
 
   R vdotBL = vxL * BxL + vyL * ByL;
   Flux5<R> FL, FR;
@@ -414,12 +439,16 @@ __device__ __forceinline__ Flux5<R> hlld(R gamma, R rhoL, R rhoR, R vxL, R vxR, 
   return hlld_guard(F, SL, SR, FL, FR, rhoL, rhoR, vxL, vxR, vyL, vyR, enL, enR, ByL, ByR, dM, dMn, dMt, dE, dB);
 }
 
+// rcp_gm1: RN(1/(gamma - 1)) for div_by, or 0.  HLLE keeps IEEE division: with
+// div_by its FP64 stage-3 kernel spilled 32 / 84 bytes per thread instead of
+// 20 / 36 and ran 0.1% slower on the rotor; Rusanov and HLLD gain.
 template <typename R, int SOLVER>
 __device__ __forceinline__ Flux5<R> riemann(R gamma, R rL, R rR, R uL, R uR, R vL, R vR, R PL, R PR,
-                                            R BnL, R BnR, R BtL, R BtR) {
-  if (SOLVER == RIEMANN_RUSANOV) return rusanov<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR);
+                                            R BnL, R BnR, R BtL, R BtR, double rcp_gm1 = 0.0) {
+  if (SOLVER == RIEMANN_RUSANOV)
+    return rusanov<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR, rcp_gm1);
   if (SOLVER == RIEMANN_HLLE) return hlle<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR);
-  return hlld<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR);
+  return hlld<R>(gamma, rL, rR, uL, uR, vL, vR, PL, PR, BnL, BnR, BtL, BtR, rcp_gm1);
 }
 
 // src/mhd_change_states.f90:116-166 (apply_conserved_floors), one cell.

@@ -149,6 +149,8 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   g.vol = cfg->dx * cfg->dy;
   g.len = (cfg->dx < cfg->dy) ? cfg->dx : cfg->dy;
   g.inv_vol = 1.0 / g.vol;
+  g.rcp_vol = shared_reciprocal(g.vol);
+  g.rcp_gm1 = shared_reciprocal(cfg->gamma - 1.0);
   g.courant = cfg->courant;
   g.t_out = cfg->t_out;
   g.t_end = cfg->t_end;

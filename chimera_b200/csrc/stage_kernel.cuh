@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     }
     const R gamma = R(g.gamma);
     const R vol = R(g.vol);
+    const double rcp_vol = g.rcp_vol, rcp_gm1 = g.rcp_gm1;
     const R dt = R(ctl->dt);
     const int sbuf = ctl->parity, obuf = 1 - sbuf;
     const int in_buf = (STAGE == 1) ? sbuf : (STAGE == 2 ? obuf : 2);
@@ -390,7 +391,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
               sU[3 * (TX * TY) + c] = c3;
             }
           }
-          Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol);
+          Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol, rcp_vol);
           sP[0 * G::NP + p] = pr.rho;
           sP[1 * G::NP + p] = pr.vx;
           sP[2 * G::NP + p] = pr.vy;
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             sU[3 * (TX * TY) + c] = c3;
           }
         }
-        Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol);
+        Prim<R> pr = get_primitive<R>(c0, c1, c2, c3, Bx, By, gamma, vol, rcp_vol);
         sP[0 * G::NP + p] = pr.rho;
         sP[1 * G::NP + p] = pr.vx;
         sP[2 * G::NP + p] = pr.vy;
@@ -518,7 +519,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
       const R utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
       const R bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
       const R btL = ydir ? L[4] : L[5], btR = ydir ? Rv[4] : Rv[5];
-      Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR);
+      Flux5<R> F = riemann<R, SOLVER>(gamma, L[0], Rv[0], unL, unR, utL, utR, L[3], Rv[3], bnL, bnR, btL, btR,
+                                      rcp_gm1);
       R* dst = ydir ? sFy : sFx;
       const int NF = ydir ? G::NFY : G::NFX;
       dst[0 * NF + ff] = F.mass;
@@ -675,7 +677,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         const double Bx = hx ? 0.5 * (double(bxn) + double(bxm)) : double(bxn);
         const double By = hy ? 0.5 * (double(byn) + double(bym)) : double(byn);
         Prim<double> pr = get_primitive<double>(double(U[0]), double(U[1]), double(U[2]), double(U[3]),
-                                                Bx, By, g.gamma, g.vol);
+                                                Bx, By, g.gamma, g.vol, g.rcp_vol);
         e_speed = run_max(e_speed, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
         const double d = fabs(divb_cell(double(bxn), double(bxm), double(byn), double(bym), hx, hy,
                                         g.inv_dx, g.inv_dy, g.square != 0));
@@ -751,7 +753,7 @@ __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
         const double Bx = hx ? 0.5 * (bxc + bxm) : bxc;
         const double By = hy ? 0.5 * (byc + bym) : byc;
         Prim<double> pr = get_primitive<double>(double(in[0][k]), double(in[1][k]), double(in[2][k]),
-                                                double(in[3][k]), Bx, By, g.gamma, g.vol);
+                                                double(in[3][k]), Bx, By, g.gamma, g.vol, g.rcp_vol);
         sp = run_max(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
         bmx = run_max(bmx, sqrt(Bx * Bx + By * By));
       }

@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         if (sj > 0) By = 0.5 * (byc + src[5][idx - nx]);
         else By = py ? 0.5 * (byc + src[5][idx + size_t(ny - 1) * nx]) : byc;
         const Prim<double> pd = get_primitive<double>(src[0][idx], src[1][idx], src[2][idx], src[3][idx], Bx, By,
-                                                      g.gamma, g.vol);
+                                                      g.gamma, g.vol, g.rcp_vol);
         sP[0 * G::NP + p] = float(pd.rho);
         sP[1 * G::NP + p] = float(pd.vx);
         sP[2 * G::NP + p] = float(pd.vy);
@@ -664,7 +664,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
             const bool hx = (i > 0) || px, hy = (j > 0) || py;
             const double Bx = hx ? 0.5 * (bxn + bxm) : bxn;
             const double By = hy ? 0.5 * (byn + bym) : byn;
-            const Prim<double> pr = get_primitive<double>(U[0], U[1], U[2], U[3], Bx, By, g.gamma, g.vol);
+            const Prim<double> pr = get_primitive<double>(U[0], U[1], U[2], U[3], Bx, By, g.gamma, g.vol, g.rcp_vol);
             e_speed = run_max(e_speed, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
             const double dv = fabs(divb_cell(bxn, bxm, byn, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
             e_dmax = run_max(e_dmax, dv);

@@ -1,7 +1,10 @@
-"""Evidence for an FP64 division through a shared, correctly rounded
-reciprocal plus one Markstein correction step: it must reproduce IEEE
-division bit for bit on random quotients (tests/numerics/div_sweep.c).  The
-default sweep is 1.6e7 quotients; CHIMERA_DIV_SWEEP_SCALE=100 runs 1.6e9."""
+"""The FP64 division through a reciprocal fixed for the launch (div_by in
+chimera_b200/csrc/mhd_device.cuh: one Markstein correction step inside its
+exact range, IEEE division outside it) must reproduce IEEE division bit for
+bit (tests/numerics/div_sweep.c mirrors it on the host): random quotients,
+quotients within a few 2^-106 of a rounding midpoint, and the numerators at
+the ends of the range.  The default sweep is about 2.4e7 quotients;
+CHIMERA_DIV_SWEEP_SCALE=100 runs about 2.4e9."""
 import os
 import shutil
 import subprocess
@@ -19,7 +22,8 @@ def test_shared_reciprocal_division_matches_ieee(tmp_path):
     subprocess.run([cc, "-O2", "-ffp-contract=off", "-o", str(exe), os.path.join(HERE, "numerics", "div_sweep.c"),
                     "-lm"], check=True)
     scale = int(os.environ.get("CHIMERA_DIV_SWEEP_SCALE", "1"))
-    out = subprocess.run([str(exe), str(1000000 * scale), "100", str(100000 * scale)], capture_output=True,
-                         text=True, check=True, timeout=3600).stdout.split()
+    out = subprocess.run([str(exe), str(1000000 * scale), "100", str(100000 * scale), str(4000000 * scale)],
+                         capture_output=True, text=True, check=True, timeout=3600).stdout.split()
     total, bad = int(out[0]), int(out[1])
-    assert total == 16000000 * scale and bad == 0
+    # 13 fixed and 100 random denominators, most of the near-midpoint draws, the range ends
+    assert total > 23000000 * scale and bad == 0
