@@ -423,7 +423,8 @@ def run_chimera(args, world, rank, local):
         e2e = {"value": world * cells * k2 / (ms2 * 1e-3), "unit": "zone-cycles/s",
                "h2d_bytes_per_step": 6 * 8 * cells, "d2h_bytes_per_step": 6 * 8 * cells,
                "steps": k2, "mode": "state copied host->device and back around every RK3 step "
-                       "(chimera_step_host: stage 3's finished row bands go back while later bands compute)"}
+                       "(chimera_step_host: the three stages run as a wavefront over chunks of tile rows "
+                       "and each finished chunk goes back while later chunks compute)"}
 
     kh = adj_leg = None
     if world == 1 and args.kh == "on":

@@ -119,10 +119,17 @@ struct chimera_handle {
   char* d_tmaps = nullptr;           // [TMA variant slot][member][buffer 3][field 6] tensor maps
   std::vector<int> tmap_slot;        // per variant: its slot in d_tmaps, -1 without TMA
   std::vector<unsigned char> tmap_ok;   // [slot][member]: the member's maps exist
-  cudaStream_t copy_stream = nullptr;   // chimera_step_host: device-to-host copies of finished bands
-  // chimera_step_host: stage-3 band b written.  Four bands: each extra
-  // device-to-host copy costs about 3 us, against the compute of one band
-  cudaEvent_t band_done[4] = {};
+  // chimera_step_host: U^{n+1} goes back in chunks of tile rows on
+  // copy_stream while the later chunks compute; stages 2 and 3 run on
+  // band_stream[0] / [1] so that the chunks' partial waves of CTAs overlap.
+  // s1_done / s2_done / band_done: chunk k of stage 1 / 2 / 3 written.
+  static constexpr int kChunks = 10;
+  cudaStream_t copy_stream = nullptr;
+  cudaStream_t band_stream[2] = {};
+  cudaEvent_t s1_done[kChunks] = {};
+  cudaEvent_t s2_done[kChunks] = {};
+  cudaEvent_t band_done[kChunks] = {};
+  cudaEvent_t band_join = nullptr;
   double* d_stage64 = nullptr;       // FP64 staging for FP32-bulk set/get
   size_t max_cells = 0;
   std::vector<bool> dt_valid;        // per member: Control::dt matches the state
@@ -193,7 +200,8 @@ static void harvest_profile(chimera_handle* h) {
   h->timed.clear();
 }
 
-static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_begin, int w_end);
+static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_begin, int w_end,
+                      cudaStream_t stream = nullptr);
 
 // kind: 0 = CFL kernel, 1..3 = stage kernels
 static int launch(chimera_handle* h, const KernelEntry& k, int grid, int kind) {
@@ -211,7 +219,9 @@ static int launch(chimera_handle* h, const KernelEntry& k, int grid, int kind) {
   return rc;
 }
 
-static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_begin, int w_end) {
+// stream: the handle's stream unless given
+static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_begin, int w_end,
+                      cudaStream_t stream) {
   StageArgs a;
   a.members = h->d_members;
   a.ctl = h->d_ctl;
@@ -226,7 +236,7 @@ static int launch_raw(chimera_handle* h, const KernelEntry& k, int grid, int w_b
   a.counters = h->counters;
   a.dry = h->dry;
   void* args[] = {&a};
-  CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.nt), args, k.smem, h->stream));
+  CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.nt), args, k.smem, stream ? stream : h->stream));
   return CHIMERA_OK;
 }
 
@@ -593,6 +603,13 @@ void chimera_destroy(chimera_handle* h) {
   cudaFree(h->d_tmaps);
   for (auto e : h->band_done)
     if (e) cudaEventDestroy(e);
+  for (auto e : h->s1_done)
+    if (e) cudaEventDestroy(e);
+  for (auto e : h->s2_done)
+    if (e) cudaEventDestroy(e);
+  if (h->band_join) cudaEventDestroy(h->band_join);
+  for (auto st : h->band_stream)
+    if (st) cudaStreamDestroy(st);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   cudaGetLastError();
@@ -734,9 +751,10 @@ int chimera_step_host(chimera_handle* h, const double* const* in, double* const*
   const chimera_cfg& cf = h->cfg[0];
   const Member& g = h->hm[0];
   h->dt_valid[0] = false;
-  // Everything issued here is asynchronous, on the handle's stream and the
-  // copy stream; the exit below drains both, so that no copy from in[] or into
-  // out[] outlives the call, on the error paths too.
+  // Everything issued here is asynchronous, on the handle's stream, the two
+  // wavefront streams and the copy stream; the exit below drains all four, so
+  // that no copy from in[] or into out[] outlives the call, on the error paths
+  // too.
   auto issue = [&]() -> int {
     for (int q = 0; q < 6; ++q) {
       const int e = copy_field_in(h, 0, g.buf[c.parity][q], in[q], ld, CHIMERA_HOST);
@@ -750,35 +768,88 @@ int chimera_step_host(chimera_handle* h, const double* const* in, double* const*
       return CHIMERA_OK;
     }
     int e = ensure_dt(h);
-    for (int s = 0; s < 2 && !e; ++s) e = launch(h, h->ks.stage[h->riemann - 1][s], h->grid_stage[s], s + 1);
     if (e) return e;
     if (!h->copy_stream) {
       CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-      for (auto& ev : h->band_done) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      for (auto& st : h->band_stream) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      for (auto* evs : {h->s1_done, h->s2_done, h->band_done})
+        for (int k = 0; k < chimera_handle::kChunks; ++k) CK(cudaEventCreateWithFlags(&evs[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h->band_join, cudaEventDisableTiming));
     }
-    // bands of tile rows (work items are row-major within the grid)
+    // Chunks of tile rows (work items are row-major within the grid) that
+    // double in size -- 1, 2, 4, ... tile rows, the last one taking a remainder
+    // smaller than itself -- so that the first rows go back early and later
+    // chunks need few copies.  A tile reads rows
+    // [j0 - 3, j0 + TY + 2) of its stage's input: tile row r of a stage needs
+    // tile rows r - 1 .. r + 1 of the stage before it.
     const int ty = h->ks.stage[0][0].ty;
-    const int rows = g.tiles_y, nb = std::min(rows, int(sizeof(h->band_done) / sizeof(h->band_done[0])));
+    const int rows = g.tiles_y;
+    int end[chimera_handle::kChunks], nc = 0;   // chunk k: tile rows [end[k - 1], end[k])
+    for (int r = 1;; r = 2 * r + 1) {
+      const int prev = nc ? end[nc - 1] : 0;
+      const bool last = rows - r < r - prev || nc == chimera_handle::kChunks - 1;
+      end[nc++] = last ? rows : r;
+      if (last) break;
+    }
     const int out_buf = 1 - c.parity;   // stage 3 writes U^{n+1} there; the finish flips the parity
-    const KernelEntry& k3 = h->ks.stage[h->riemann - 1][2];
-    for (int b = 0; b < nb; ++b) {
-      const int r0 = rows * b / nb, r1 = rows * (b + 1) / nb;
+    const size_t w = size_t(cf.nx) * sizeof(double);
+    const KernelEntry* ks = h->ks.stage[h->riemann - 1];
+    // stage s over tile rows [r0, r1) on stream st (nothing for an empty range)
+    auto rows_launch = [&](int s, int r0, int r1, cudaStream_t st) -> int {
+      r0 = std::max(r0, 0);
+      r1 = std::min(r1, rows);
+      if (r1 <= r0) return CHIMERA_OK;
       const int w0 = r0 * g.tiles_x, w1 = r1 * g.tiles_x;
-      const int grid = std::max(1, std::min(h->grid_stage[2], w1 - w0));
-      e = launch_raw(h, k3, grid, w0, w1);
-      if (e) return e;
-      CK(cudaEventRecord(h->band_done[b], h->stream));
-      CK(cudaStreamWaitEvent(h->copy_stream, h->band_done[b], 0));
-      const int y0 = r0 * ty, y1 = std::min(r1 * ty, cf.ny);
-      const size_t w = size_t(cf.nx) * sizeof(double);
+      return launch_raw(h, ks[s], std::max(1, std::min(h->grid_stage[s], w1 - w0)), w0, w1, st);
+    };
+    // stage 3 over chunk k, then its rows of the six fields back to the host
+    auto finish_chunk = [&](int k, cudaStream_t st) -> int {
+      const int r0 = k ? end[k - 1] : 0;
+      const int e3 = rows_launch(2, r0, end[k], st);
+      if (e3) return e3;
+      CK(cudaEventRecord(h->band_done[k], st));
+      CK(cudaStreamWaitEvent(h->copy_stream, h->band_done[k], 0));
+      const int y0 = r0 * ty, y1 = std::min(end[k] * ty, cf.ny);
       for (int q = 0; q < 6; ++q)
         CK(cudaMemcpy2DAsync(out[q] + size_t(y0) * ld, size_t(ld) * sizeof(double),
                              static_cast<const char*>(g.buf[out_buf][q]) + size_t(y0) * w, w, w, y1 - y0,
                              cudaMemcpyDeviceToHost, h->copy_stream));
+      return CHIMERA_OK;
+    };
+    if (!g.periodic_y) {
+      // a wavefront: stage 1 runs two tile rows ahead of stage 3 on the
+      // handle's stream, stage 2 one row ahead on band_stream[0], stage 3 on
+      // band_stream[1].  Stage 3 writes U^{n+1} over U1's rows of chunk k only
+      // after stage 2 has finished the tile row above the chunk, the last
+      // reader of those rows; later stage-2 rows read none of them.
+      cudaStream_t s2 = h->band_stream[0], s3 = h->band_stream[1];
+      int d1 = 0, d2 = 0;   // stage 1 / 2 issued for tile rows [0, d1) / [0, d2)
+      for (int k = 0; k < nc; ++k) {
+        const int t1 = std::min(end[k] + 2, rows), t2 = std::min(end[k] + 1, rows);
+        if ((e = rows_launch(0, d1, t1, h->stream))) return e;
+        d1 = std::max(d1, t1);
+        CK(cudaEventRecord(h->s1_done[k], h->stream));
+        CK(cudaStreamWaitEvent(s2, h->s1_done[k], 0));
+        if ((e = rows_launch(1, d2, t2, s2))) return e;
+        d2 = std::max(d2, t2);
+        CK(cudaEventRecord(h->s2_done[k], s2));
+        CK(cudaStreamWaitEvent(s3, h->s2_done[k], 0));
+        if ((e = finish_chunk(k, s3))) return e;
+      }
+      // later work on the handle's stream comes after the wavefront
+      CK(cudaEventRecord(h->band_join, s3));
+      CK(cudaStreamWaitEvent(h->stream, h->band_join, 0));
+    } else {   // y-periodic: tile row 0 reads the last row, so stages 1 and 2 take the whole grid
+      for (int s = 0; s < 2; ++s)
+        if ((e = launch(h, ks[s], h->grid_stage[s], s + 1))) return e;
+      for (int k = 0; k < nc; ++k)
+        if ((e = finish_chunk(k, h->stream))) return e;
     }
     return CHIMERA_OK;
   };
   rc = issue();
+  for (auto st : h->band_stream)
+    if (st) cudaStreamSynchronize(st);
   const cudaError_t e_copy = h->copy_stream ? cudaStreamSynchronize(h->copy_stream) : cudaSuccess;
   const cudaError_t e_main = cudaStreamSynchronize(h->stream);
   if (rc) { cudaGetLastError(); return rc; }

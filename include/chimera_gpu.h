@@ -114,9 +114,10 @@ int chimera_get_state(chimera_handle* h, double* Mass, double* Momx, double* Mom
 /* One RK3 step on HOST arrays: in[6] (Mass, Momx, Momy, Energy, b_x, b_y,
  * pitch ld doubles) is copied in, advanced one step (CFL dt of the new state,
  * tOut clip, three stages) and copied out to out[6] (which may be in).  For a
- * single-grid FP64 handle the device-to-host copy of each band of rows starts
- * as soon as stage 3 has written it, overlapping the rest of the stage; pinned
- * host memory is needed for that overlap.  Synchronises.  Replaces, for a
+ * single-grid FP64 handle the stages run over chunks of rows, and the
+ * device-to-host copy of each chunk starts as soon as stage 3 has written it,
+ * overlapping the later chunks' compute; pinned host memory is needed for that
+ * overlap.  Synchronises.  Replaces, for a
  * caller that keeps its state in host arrays, one pass of the loop body of
  * src/main.f90:65-303 between the module arrays. */
 int chimera_step_host(chimera_handle* h, const double* const* in, double* const* out, int ld);

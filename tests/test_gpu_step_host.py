@@ -1,6 +1,8 @@
-"""chimera_step_host: one step on host arrays, with the device-to-host copy of
-stage 3's finished row bands overlapping the rest of the stage.  It must give
-exactly what set_state + step + get_state give."""
+"""chimera_step_host: one step on host arrays, in row bands -- the inputs land
+band by band under the CFL kernel, the stages run as a wavefront over the
+bands (stage 1 on band k, stage 2 on k - 1, stage 3 on k - 2) where y is not
+periodic, and stage 3's finished bands go back while later bands compute.  It
+must give exactly what set_state + step + get_state give."""
 import numpy as np
 import pytest
 import torch
@@ -33,10 +35,10 @@ def _pinned(arrays):
     return [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in arrays]
 
 
-@pytest.mark.parametrize("case", ["rotor128", "ragged50x37", "ot96"])
+@pytest.mark.parametrize("case", ["rotor128", "rotor512", "ragged50x37", "ot96"])
 def test_step_host_equals_set_step_get(G, case):
-    if case == "rotor128":
-        cfg, st = P.rotor(128)
+    if case.startswith("rotor"):
+        cfg, st = P.rotor(int(case[5:]))
     elif case == "ragged50x37":
         cfg, st = P.orszag_tang(50)
         cfg = cfg.replace(bc=(BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW))
