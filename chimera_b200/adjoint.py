@@ -11,7 +11,7 @@ function of the state, so the derivative of the CFL reduction is not taken;
 obtain the dt sequence from a primal run (``cfl_dts``) and reuse it.  The MOOD,
 floor and thermal-check decisions and the limiter branches are the forward's;
 at a kink the derivative is that of the branch the forward took (one-sided).
-Periodic boundaries.
+Periodic or outflow sides (each pair of opposite sides alike).
 
 Forward precision: FP64 (the tape kernels, bit-identical to the fused FP64
 step) or a reduced form -- ``FP32_BULK`` or ``FP32_MIXED`` -- in which the
@@ -29,7 +29,7 @@ import ctypes as C
 import torch
 
 from . import gpu
-from .config import FP32_BULK, FP32_MIXED, FP64, SolverConfig
+from .config import BC_PERIODIC, FP32_BULK, FP32_MIXED, FP64, SolverConfig
 
 _bound = False
 
@@ -57,7 +57,7 @@ def _ptr6(ts):
 
 
 class Adjoint:
-    """Handle for the adjoint kernels of one periodic grid (FP64)."""
+    """Handle for the adjoint kernels of one grid (FP64; periodic or outflow sides)."""
 
     def __init__(self, cfg: SolverConfig):
         self.cfg = cfg.replace(precision=FP64)
@@ -187,11 +187,22 @@ def run(adj: Adjoint, U0, dts, K: int = 20, precision: int = FP64):
 
 # --- helpers for losses on primitive inputs ------------------------------------
 
-def conserved_from_primitive(cfg: SolverConfig, rho, vx, vy, p_thermal, b_x, b_y):
-    """Torch version of get_conserved (src/mhd_change_states.f90:16-58) with the
-    cell-centred B of face B (periodic), differentiable in every input."""
+def _cell_B(cfg: SolverConfig, b_x, b_y):
+    """average_face_to_cell_B (src/mhd_field_ops.f90:120-156): the mean of a
+    cell's two faces; at a non-periodic low side the face value itself."""
     Bx = 0.5 * (b_x + torch.roll(b_x, 1, dims=1))
     By = 0.5 * (b_y + torch.roll(b_y, 1, dims=0))
+    if cfg.bc[0] != BC_PERIODIC:
+        Bx = torch.cat([b_x[:, :1], Bx[:, 1:]], dim=1)
+    if cfg.bc[2] != BC_PERIODIC:
+        By = torch.cat([b_y[:1, :], By[1:, :]], dim=0)
+    return Bx, By
+
+
+def conserved_from_primitive(cfg: SolverConfig, rho, vx, vy, p_thermal, b_x, b_y):
+    """Torch version of get_conserved (src/mhd_change_states.f90:16-58) with the
+    cell-centred B of face B, differentiable in every input."""
+    Bx, By = _cell_B(cfg, b_x, b_y)
     vol = cfg.dx * cfg.dy
     P = p_thermal + 0.5 * (Bx * Bx + By * By)
     rho_cp = torch.clamp(rho, min=1.0e-12)
@@ -203,8 +214,6 @@ def conserved_from_primitive(cfg: SolverConfig, rho, vx, vy, p_thermal, b_x, b_y
 
 
 def magnetic_energy(cfg: SolverConfig, U):
-    """sum 1/2 |B|^2 vol over cells, B cell centred from the faces (periodic)."""
-    b_x, b_y = U[4], U[5]
-    Bx = 0.5 * (b_x + torch.roll(b_x, 1, dims=1))
-    By = 0.5 * (b_y + torch.roll(b_y, 1, dims=0))
+    """sum 1/2 |B|^2 vol over cells, B cell centred from the faces."""
+    Bx, By = _cell_B(cfg, U[4], U[5])
     return 0.5 * torch.sum(Bx * Bx + By * By) * (cfg.dx * cfg.dy)

@@ -28,7 +28,13 @@
 // with forward-mode dual numbers (dual.cuh): at a kink (limiter branch, min /
 // max, floor) the derivative is that of the branch the forward took.
 //
-// Boundary conditions: periodic on all sides (outflow is rejected).
+// Boundary conditions: periodic or outflow (zero-gradient ghost cells) in x
+// and in y, each pair of opposite sides alike.  At an outflow side the forward
+// takes the nearest cell for every ghost position (src/mhd_bc.f90:36-121), the
+// outflow face->cell B (src/mhd_field_ops.f90:120-156), curl copy
+// (src/mhd_flux.f90:79-136), update without the incoming face
+// (src/mhd_flux.f90:20-76) and boundary flux correction (src/main.f90:118-148);
+// the reverse gathers transpose each of them.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -48,9 +54,15 @@ struct AdjGeom {
   int nx, ny;
   double dx, dy, inv_dx, inv_dy, inv_2dx, inv_2dy, hx, hy, gamma, vol;
   int riemann, limiter, slope, mood;
+  int px, py;   // periodic in x / y (else outflow)
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+// the cell a ghost position i (one or two cells beyond the grid) takes its
+// value from: periodic wrap, or the nearest cell (outflow)
+__device__ __forceinline__ int src(int i, int n, int periodic) {
+  return periodic ? wrap(i, n) : (i < 0 ? 0 : (i >= n ? n - 1 : i));
+}
 
 // ---------------------------------------------------------------------------
 // forward tape kernels
@@ -69,8 +81,9 @@ __global__ void k_tape_prims(AdjGeom g, const double* const* __restrict__ U, Sta
   const int n = g.nx * g.ny;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int i = c % g.nx, j = c / g.nx;
-    const double Bx = 0.5 * (U[4][c] + U[4][j * g.nx + wrap(i - 1, g.nx)]);
-    const double By = 0.5 * (U[5][c] + U[5][wrap(j - 1, g.ny) * g.nx + i]);
+    // average_face_to_cell_B: at an outflow low side the face value itself
+    const double Bx = (i > 0 || g.px) ? 0.5 * (U[4][c] + U[4][j * g.nx + wrap(i - 1, g.nx)]) : U[4][c];
+    const double By = (j > 0 || g.py) ? 0.5 * (U[5][c] + U[5][wrap(j - 1, g.ny) * g.nx + i]) : U[5][c];
     Prim<double> p = get_primitive<double>(U[0][c], U[1][c], U[2][c], U[3][c], Bx, By, g.gamma, g.vol);
     t.P[0][c] = p.rho; t.P[1][c] = p.vx; t.P[2][c] = p.vy;
     t.P[3][c] = p.P; t.P[4][c] = p.Bx; t.P[5][c] = p.By;
@@ -136,24 +149,27 @@ __device__ __forceinline__ void face_states(const AdjGeom& g, const StageTape& t
 // neighbour indices for the face with low cell (i, j) in direction ydir
 struct FaceIdx {
   int a, b, am, bp, axp, axm, ayp, aym;
+  bool b_real;   // the high cell is a cell of the grid (not the ghost past an outflow side)
 };
 __device__ __forceinline__ FaceIdx face_idx(const AdjGeom& g, int i, int j, bool ydir) {
   FaceIdx f;
   const int nx = g.nx, ny = g.ny;
   f.a = j * nx + i;
   if (!ydir) {
-    f.b = j * nx + wrap(i + 1, nx);
-    f.am = j * nx + wrap(i - 1, nx);
-    f.bp = j * nx + wrap(i + 2, nx);
+    f.b = j * nx + src(i + 1, nx, g.px);
+    f.am = j * nx + src(i - 1, nx, g.px);
+    f.bp = j * nx + src(i + 2, nx, g.px);
+    f.b_real = g.px || i + 1 < nx;
   } else {
-    f.b = wrap(j + 1, ny) * nx + i;
-    f.am = wrap(j - 1, ny) * nx + i;
-    f.bp = wrap(j + 2, ny) * nx + i;
+    f.b = src(j + 1, ny, g.py) * nx + i;
+    f.am = src(j - 1, ny, g.py) * nx + i;
+    f.bp = src(j + 2, ny, g.py) * nx + i;
+    f.b_real = g.py || j + 1 < ny;
   }
-  f.axp = j * nx + wrap(i + 1, nx);
-  f.axm = j * nx + wrap(i - 1, nx);
-  f.ayp = wrap(j + 1, ny) * nx + i;
-  f.aym = wrap(j - 1, ny) * nx + i;
+  f.axp = j * nx + src(i + 1, nx, g.px);
+  f.axm = j * nx + src(i - 1, nx, g.px);
+  f.ayp = src(j + 1, ny, g.py) * nx + i;
+  f.aym = src(j - 1, ny, g.py) * nx + i;
   return f;
 }
 
@@ -188,10 +204,35 @@ __device__ __forceinline__ double Ez_at(const AdjGeom& g, const StageTape& t, in
   i = wrap(i, nx);
   j = wrap(j, ny);
   const double fa = t.Fx[4][j * nx + i];
-  const double up = t.Fx[4][wrap(j + 1, ny) * nx + i];
+  const double up = (j == ny - 1 && !g.py) ? fa : t.Fx[4][wrap(j + 1, ny) * nx + i];   // outflow: zero gradient
   const double fb = t.Fy[4][j * nx + i];
-  const double right = t.Fy[4][j * nx + wrap(i + 1, nx)];
+  const double right = (i == nx - 1 && !g.px) ? fb : t.Fy[4][j * nx + wrap(i + 1, nx)];
   return 0.25 * (((-fa - up) + fb) + right);
+}
+
+// Outflow boundary flux correction (src/main.f90:118-148): a cell on an
+// outflow low side gets dt*dx times the physical flux of its own stage
+// primitives, in x (sx) and / or in y (sy).  Same operations as the fused
+// stage kernel's; R = double in the tape, dual numbers in the reverse sweep.
+template <typename R>
+__device__ __forceinline__ void outflow_correction(bool sx, bool sy, R ax, R ay, R gamma, R cr, R cu, R cv, R cP,
+                                                   R cBx, R cBy, R* U) {
+  if (sx) {
+    const R hb = R(0.5) * (cBx * cBx + cBy * cBy);
+    const R en = ((cP - hb) / (gamma - R(1)) + R(0.5) * cr * (cu * cu + cv * cv)) + hb;
+    U[0] = U[0] + ax * cr * cu;
+    U[1] = U[1] + ax * ((cr * (cu * cu) + cP) - cBx * cBx);
+    U[2] = U[2] + ax * (cr * cu * cv - cBx * cBy);
+    U[3] = U[3] + ax * ((en + cP) * cu - cBx * (cBx * cu + cBy * cv));
+  }
+  if (sy) {
+    const R hb = R(0.5) * (cBx * cBx + cBy * cBy);
+    const R en = ((cP - hb) / (gamma - R(1)) + R(0.5) * cr * (cu * cu + cv * cv)) + hb;
+    U[0] = U[0] + ay * cr * cv;
+    U[2] = U[2] + ay * ((cr * (cv * cv) + cP) - cBy * cBy);
+    U[1] = U[1] + ay * (cr * cv * cu - cBy * cBx);
+    U[3] = U[3] + ay * ((en + cP) * cv - cBy * (cBy * cv + cBx * cu));
+  }
 }
 
 __global__ void k_tape_update(AdjGeom g, int stage, double dt, const double* const* __restrict__ Uin,
@@ -204,16 +245,26 @@ __global__ void k_tape_update(AdjGeom g, int stage, double dt, const double* con
     double U[4];
     for (int q = 0; q < 4; ++q) {
       double F = Uin[q][c];
-      F = (F - ax * t.Fx[q][c]) + ax * t.Fx[q][cxm];
-      F = (F - ay * t.Fy[q][c]) + ay * t.Fy[q][cym];
+      // at an outflow low side the incoming face flux is left out
+      if (i > 0 || g.px) F = (F - ax * t.Fx[q][c]) + ax * t.Fx[q][cxm];
+      else F = F - ax * t.Fx[q][c];
+      if (j > 0 || g.py) F = (F - ay * t.Fy[q][c]) + ay * t.Fy[q][cym];
+      else F = F - ay * t.Fy[q][c];
       U[q] = F;
       t.Upre[q][c] = F;
     }
     const double Bx = t.P[4][c], By = t.P[5][c];
     conserved_floors<double>(U[0], U[1], U[2], U[3], Bx, By, g.gamma, g.vol);
+    outflow_correction<double>(!g.px && i == 0, !g.py && j == 0, ax, ay, g.gamma, t.P[0][c], t.P[1][c], t.P[2][c],
+                               t.P[3][c], Bx, By, U);
     const double e0 = Ez_at(g, t, i, j);
-    double bx = Uin[4][c] + dt * (((-e0) - (-Ez_at(g, t, i, j - 1))) * g.inv_dy);
-    double by = Uin[5][c] + dt * (-(((-e0) - (-Ez_at(g, t, i - 1, j))) * g.inv_dx));
+    // curl of -Ez; at an outflow low side the second row / column's difference
+    const double dbx = (j > 0 || g.py) ? ((-e0) - (-Ez_at(g, t, i, j - 1))) * g.inv_dy
+                                       : ((-Ez_at(g, t, i, 1)) - (-e0)) * g.inv_dy;
+    const double dby = (i > 0 || g.px) ? -(((-e0) - (-Ez_at(g, t, i - 1, j))) * g.inv_dx)
+                                       : -(((-Ez_at(g, t, 1, j)) - (-e0)) * g.inv_dx);
+    double bx = Uin[4][c] + dt * dbx;
+    double by = Uin[5][c] + dt * dby;
     if (stage == 2) {
       for (int q = 0; q < 4; ++q) U[q] = 0.75 * U0[q][c] + 0.25 * U[q];
       bx = 0.75 * U0[4][c] + 0.25 * bx;
@@ -246,6 +297,7 @@ struct RevBuf {
   double* w[24];     // per cell, field q, dir d: wL, wR at index (q*2+d)*2 + {0,1}
   double* lPc[6];    // direct face adjoints to each cell's primitives
   double* lB2[2];    // adjoint of cell Bx, By (for the face->cell average)
+  double* lPcor[6];  // adjoint of a cell's primitives through the outflow flux correction
 };
 
 // floors Jacobian-transpose product at inputs (M, Mx, My, E) with cell B
@@ -264,8 +316,8 @@ __device__ __forceinline__ void floors_vjp(const AdjGeom& g, const double* Uin4,
   }
 }
 
-__global__ void k_rev_cells1(AdjGeom g, int stage, const StageTape t, const double* const* __restrict__ lout,
-                             RevBuf r, double* const* __restrict__ lU0acc) {
+__global__ void k_rev_cells1(AdjGeom g, int stage, double stage_dt, const StageTape t,
+                             const double* const* __restrict__ lout, RevBuf r, double* const* __restrict__ lU0acc) {
   const int n = g.nx * g.ny;
   const double c0 = (stage == 2) ? 0.75 : (1.0 / 3.0);
   const double c1 = (stage == 2) ? 0.25 : (2.0 / 3.0);
@@ -292,6 +344,25 @@ __global__ void k_rev_cells1(AdjGeom g, int stage, const StageTape t, const doub
       lbp0 = lout[4][c];
       lbp1 = lout[5][c];
     }
+    // outflow flux correction (added after the first floors): lpp is the
+    // adjoint of the correction too; through it to the cell's stage primitives
+    const int i = c % g.nx, j = c / g.nx;
+    const bool sx = !g.px && i == 0, sy = !g.py && j == 0;
+    double lcor[6] = {0, 0, 0, 0, 0, 0};
+    if (sx || sy) {
+      using D = Dual<6>;
+      const double ax = stage_dt * g.dy, ay = stage_dt * g.dx;
+      D pv[6];
+      for (int k = 0; k < 6; ++k) pv[k] = seed<6>(t.P[k][c], k);
+      D U[4] = {D(0.0), D(0.0), D(0.0), D(0.0)};
+      outflow_correction<D>(sx, sy, D(ax), D(ay), D(g.gamma), pv[0], pv[1], pv[2], pv[3], pv[4], pv[5], U);
+      for (int k = 0; k < 6; ++k) {
+        double sacc = 0.0;
+        for (int q = 0; q < 4; ++q) sacc += lpp[q] * U[q].d[k];
+        lcor[k] = sacc;
+      }
+    }
+    for (int k = 0; k < 6; ++k) r.lPcor[k][c] = lcor[k];
     double up[4] = {t.Upre[0][c], t.Upre[1][c], t.Upre[2][c], t.Upre[3][c]};
     double lu[4];
     floors_vjp(g, up, Bx, By, lpp, lu, lB);
@@ -305,13 +376,25 @@ __global__ void k_rev_cells1(AdjGeom g, int stage, const StageTape t, const doub
 
 // lambda_Ez at corner (i+1/2, j+1/2): b_x(i,j) gets -dt/dy Ez(i,j), b_x(i,j+1)
 // gets +dt/dy Ez(i,j); b_y(i,j) gets +dt/dx Ez(i,j), b_y(i+1,j) gets -dt/dx.
+// At an outflow low side b_x(i,0) takes row 1's difference, dt/dy (Ez(i,0) -
+// Ez(i,1)), and b_y(0,j) column 1's, dt/dx (Ez(1,j) - Ez(0,j)); past an
+// outflow high side there is no b_x(i,ny) / b_y(nx,j).
 __global__ void k_rev_corners(AdjGeom g, double dt, RevBuf r) {
   const int n = g.nx * g.ny;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int i = c % g.nx, j = c / g.nx;
     const int cyp = wrap(j + 1, g.ny) * g.nx + i;
     const int cxp = j * g.nx + wrap(i + 1, g.nx);
-    r.lEz[c] = dt * g.inv_dy * (r.lbp[0][cyp] - r.lbp[0][c]) + dt * g.inv_dx * (r.lbp[1][c] - r.lbp[1][cxp]);
+    double sx = 0.0, sy = 0.0;
+    if (j + 1 < g.ny || g.py) sx += r.lbp[0][cyp];
+    if (j > 0 || g.py) sx -= r.lbp[0][c];
+    if (!g.py && j == 0) sx += r.lbp[0][i];
+    if (!g.py && j == 1) sx -= r.lbp[0][i];
+    if (i > 0 || g.px) sy += r.lbp[1][c];
+    if (i + 1 < g.nx || g.px) sy -= r.lbp[1][cxp];
+    if (!g.px && i == 0) sy -= r.lbp[1][j * g.nx];
+    if (!g.px && i == 1) sy += r.lbp[1][j * g.nx];
+    r.lEz[c] = dt * g.inv_dy * sx + dt * g.inv_dx * sy;
   }
 }
 
@@ -328,9 +411,20 @@ __global__ void k_rev_faces(AdjGeom g, double dt, StageTape t, RevBuf r) {
     // adjoint of this face's 5 fluxes (conserved ordering)
     double lF[5];
     const double wgt = ydir ? ay : ax;
-    for (int q = 0; q < 4; ++q) lF[q] = wgt * (r.lUp[q][f.b] - r.lUp[q][c]);
-    if (!ydir) lF[4] = -0.25 * (r.lEz[c] + r.lEz[wrap(j - 1, g.ny) * g.nx + i]);
-    else lF[4] = 0.25 * (r.lEz[c] + r.lEz[j * g.nx + wrap(i - 1, g.nx)]);
+    // the flux leaves cell a and enters cell b (none past an outflow high side)
+    for (int q = 0; q < 4; ++q) lF[q] = wgt * ((f.b_real ? r.lUp[q][f.b] : 0.0) - r.lUp[q][c]);
+    // Ez(i,j) = 1/4 (-Fx(i,j) - Fx(i,j+1) + Fy(i,j) + Fy(i+1,j)); at an outflow
+    // high side Fx(i,ny) / Fy(nx,j) is the face itself (zero gradient)
+    const double e0 = r.lEz[c];
+    if (!ydir) {
+      double s4 = (j > 0 || g.py) ? e0 + r.lEz[wrap(j - 1, g.ny) * g.nx + i] : e0;
+      if (j == g.ny - 1 && !g.py) s4 += e0;
+      lF[4] = -0.25 * s4;
+    } else {
+      double s4 = (i > 0 || g.px) ? e0 + r.lEz[j * g.nx + wrap(i - 1, g.nx)] : e0;
+      if (i == g.nx - 1 && !g.px) s4 += e0;
+      lF[4] = 0.25 * s4;
+    }
     // recompute the face states (values + flags), then the flux Jacobian
     double L[6], Rv[6];
     uint32_t fl;
@@ -389,14 +483,23 @@ __global__ void k_rev_slopes(AdjGeom g, StageTape t, RevBuf r) {
   const int n = g.nx * g.ny;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int i = c % g.nx, j = c / g.nx;
-    const int cxm = j * g.nx + wrap(i - 1, g.nx), cym = wrap(j - 1, g.ny) * g.nx + i;
-    const int cxp = j * g.nx + wrap(i + 1, g.nx), cyp = wrap(j + 1, g.ny) * g.nx + i;
+    const int cxm = j * g.nx + src(i - 1, g.nx, g.px), cym = src(j - 1, g.ny, g.py) * g.nx + i;
+    const int cxp = j * g.nx + src(i + 1, g.nx, g.px), cyp = src(j + 1, g.ny, g.py) * g.nx + i;
+    // at an outflow low side there is no face below the cell; past an outflow
+    // high side the ghost's value is this cell's (its slope, from two equal
+    // differences, depends on no cell)
+    const bool hx = i > 0 || g.px, hy = j > 0 || g.py;
+    const bool ex = !g.px && i == g.nx - 1, ey = !g.py && j == g.ny - 1;
     for (int q = 0; q < 6; ++q) {
       // this cell is the low cell of faces (c, x) and (c, y), the high cell of (cxm, x) and (cym, y)
-      r.lPc[q][c] = r.fX[4 * q + 0][c] + r.fY[4 * q + 0][c] + r.fX[4 * q + 2][cxm] + r.fY[4 * q + 2][cym];
+      double lv = r.fX[4 * q + 0][c] + r.fY[4 * q + 0][c] + (hx ? r.fX[4 * q + 2][cxm] : 0.0) +
+                  (hy ? r.fY[4 * q + 2][cym] : 0.0);
+      if (ex) lv += r.fX[4 * q + 2][c];
+      if (ey) lv += r.fY[4 * q + 2][c];
+      r.lPc[q][c] = lv;
       for (int d = 0; d < 2; ++d) {
-        const double ls = (d == 0) ? (r.fX[4 * q + 1][c] + r.fX[4 * q + 3][cxm])
-                                   : (r.fY[4 * q + 1][c] + r.fY[4 * q + 3][cym]);
+        const double ls = (d == 0) ? (r.fX[4 * q + 1][c] + (hx ? r.fX[4 * q + 3][cxm] : 0.0))
+                                   : (r.fY[4 * q + 1][c] + (hy ? r.fY[4 * q + 3][cym] : 0.0));
         const double fm = t.P[q][d == 0 ? cxm : cym], f0 = t.P[q][c], fp = t.P[q][d == 0 ? cxp : cyp];
         const double inv_h = d == 0 ? g.inv_dx : g.inv_dy;
         double wl, wr;
@@ -439,15 +542,24 @@ __global__ void k_rev_prims(AdjGeom g, StageTape t, RevBuf r, const double* cons
     double lP[6];
     for (int q = 0; q < 6; ++q) {
       double v = r.lPc[q][c];
-      // x slopes: s(c) uses f(c-1), f(c), f(c+1)
-      v += r.w[(q * 2 + 0) * 2 + 0][c] - r.w[(q * 2 + 0) * 2 + 1][c] - r.w[(q * 2 + 0) * 2 + 0][cxp] +
-           r.w[(q * 2 + 0) * 2 + 1][cxm];
-      v += r.w[(q * 2 + 1) * 2 + 0][c] - r.w[(q * 2 + 1) * 2 + 1][c] - r.w[(q * 2 + 1) * 2 + 0][cyp] +
-           r.w[(q * 2 + 1) * 2 + 1][cym];
+      // slopes: s(p) uses f(p-1), f(p), f(p+1).  At an outflow side the ghost
+      // beyond is this cell: at the low side s(0)'s f(-1) and f(0) terms
+      // cancel to -w1, at the high side s(nx-1)'s f(nx-1) and f(nx) terms to w0
+      for (int d = 0; d < 2; ++d) {
+        const double* w0 = r.w[(q * 2 + d) * 2 + 0];
+        const double* w1 = r.w[(q * 2 + d) * 2 + 1];
+        const bool per = d == 0 ? g.px : g.py;
+        const int k = d == 0 ? i : j, nk = d == 0 ? g.nx : g.ny;
+        const int cm = d == 0 ? cxm : cym, cp = d == 0 ? cxp : cyp;
+        if (per || (k > 0 && k < nk - 1)) v += w0[c] - w1[c] - w0[cp] + w1[cm];
+        else if (k == 0) v += (-w1[c]) - w0[cp];
+        else v += w0[c] + w1[cm];
+      }
       lP[q] = v;
     }
     lP[4] += r.lBc[0][c];
     lP[5] += r.lBc[1][c];
+    for (int q = 0; q < 6; ++q) lP[q] += r.lPcor[q][c];
     using D = Dual<6>;
     const double Bx = t.P[4][c], By = t.P[5][c];
     D M = seed<6>(Uin[0][c], 0), Mx = seed<6>(Uin[1][c], 1), My = seed<6>(Uin[2][c], 2);
@@ -472,8 +584,11 @@ __global__ void k_rev_faceB(AdjGeom g, RevBuf r, double* const* __restrict__ lin
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int i = c % g.nx, j = c / g.nx;
     const int cxp = j * g.nx + wrap(i + 1, g.nx), cyp = wrap(j + 1, g.ny) * g.nx + i;
-    lin[4][c] = r.lbp[0][c] + 0.5 * r.lB2[0][c] + 0.5 * r.lB2[0][cxp];
-    lin[5][c] = r.lbp[1][c] + 0.5 * r.lB2[1][c] + 0.5 * r.lB2[1][cyp];
+    // b_x(i) enters Bx(i) (alone at an outflow low side) and Bx(i+1) (none past the high side)
+    lin[4][c] = r.lbp[0][c] + ((i > 0 || g.px) ? 0.5 : 1.0) * r.lB2[0][c] +
+                ((i + 1 < g.nx || g.px) ? 0.5 * r.lB2[0][cxp] : 0.0);
+    lin[5][c] = r.lbp[1][c] + ((j > 0 || g.py) ? 0.5 : 1.0) * r.lB2[1][c] +
+                ((j + 1 < g.ny || g.py) ? 0.5 * r.lB2[1][cyp] : 0.0);
   }
 }
 
@@ -525,8 +640,13 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
   *out = nullptr;
   if (cfg->nx < 4 || cfg->ny < 4 || !(cfg->dx > 0) || !(cfg->dy > 0) || !(cfg->gamma > 1.0)) return CHIMERA_ERR_BAD_ARG;
   if (cfg->riemann < 1 || cfg->riemann > 3 || cfg->limiter < 1 || cfg->limiter > 2) return CHIMERA_ERR_BAD_ARG;
-  if (cfg->bc_xlo != CHIMERA_BC_PERIODIC || cfg->bc_xhi != CHIMERA_BC_PERIODIC ||
-      cfg->bc_ylo != CHIMERA_BC_PERIODIC || cfg->bc_yhi != CHIMERA_BC_PERIODIC)
+  for (int b : {cfg->bc_xlo, cfg->bc_xhi, cfg->bc_ylo, cfg->bc_yhi})
+    if (b < CHIMERA_BC_PERIODIC || b > CHIMERA_BC_INFLOW) return CHIMERA_ERR_BAD_ARG;
+  // every non-periodic kind acts as outflow (src/mhd_bc.f90:36-121); a side
+  // that wraps while its opposite side does not is not supported (as for the
+  // forward handles)
+  if ((cfg->bc_xlo == CHIMERA_BC_PERIODIC) != (cfg->bc_xhi == CHIMERA_BC_PERIODIC) ||
+      (cfg->bc_ylo == CHIMERA_BC_PERIODIC) != (cfg->bc_yhi == CHIMERA_BC_PERIODIC))
     return CHIMERA_ERR_UNSUPPORTED;
   if (cfg->precision != CHIMERA_FP64) return CHIMERA_ERR_UNSUPPORTED;
   if ((long long)cfg->nx * cfg->ny >= (1LL << 31)) return CHIMERA_ERR_TOO_LARGE;   // int cell indices
@@ -543,6 +663,8 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
   g.riemann = cfg->riemann; g.limiter = cfg->limiter;
   g.slope = cfg->use_slope_limiting ? 1 : 0;
   g.mood = cfg->mood ? 1 : 0;
+  g.px = cfg->bc_xlo == CHIMERA_BC_PERIODIC;
+  g.py = cfg->bc_ylo == CHIMERA_BC_PERIODIC;
   a->n = cfg->nx * cfg->ny;
   if (stream) a->stream = (cudaStream_t)stream;
   else {
@@ -557,8 +679,8 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
   }
   a->grid = sms * 8;
   // doubles per cell: tapes 3 x (6 P + 10 F + 4 Upre + 4 Ublend) + 2 flag words (as 1 double)
-  // + reverse (4 + 2 + 2 + 1 + 48 + 24 + 6 + 2) + U1, U2, lA, lB, lU0 (30)
-  const size_t per_cell = 3 * (24 + 1) + (4 + 2 + 2 + 1 + 48 + 24 + 6 + 2) + 30;
+  // + reverse (4 + 2 + 2 + 1 + 48 + 24 + 6 + 2 + 6) + U1, U2, lA, lB, lU0 (30)
+  const size_t per_cell = 3 * (24 + 1) + (4 + 2 + 2 + 1 + 48 + 24 + 6 + 2 + 6) + 30;
   const size_t n = size_t(a->n);
   if (cudaMalloc(&a->pool, per_cell * n * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&a->dptrs, P_COUNT * sizeof(double*)) != cudaSuccess) {
@@ -589,6 +711,7 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
   for (int q = 0; q < 24; ++q) r.w[q] = take();
   for (int q = 0; q < 6; ++q) r.lPc[q] = take();
   for (int q = 0; q < 2; ++q) r.lB2[q] = take();
+  for (int q = 0; q < 6; ++q) r.lPcor[q] = take();
   for (int q = 0; q < 6; ++q) a->U1[q] = take();
   for (int q = 0; q < 6; ++q) a->U2[q] = take();
   for (int q = 0; q < 6; ++q) a->lA[q] = take();
@@ -642,7 +765,7 @@ static void rev_stage(chimera_adjoint* a, int stage, double dt, double** in, dou
                       double** lU0) {
   const int grid = a->grid;
   StageTape& t = a->tape[stage - 1];
-  k_rev_cells1<<<grid, 256, 0, a->stream>>>(a->g, stage, t, lout, a->rev, lU0);
+  k_rev_cells1<<<grid, 256, 0, a->stream>>>(a->g, stage, dt, t, lout, a->rev, lU0);
   k_rev_corners<<<grid, 256, 0, a->stream>>>(a->g, dt, a->rev);
   k_rev_faces<SOLVER><<<grid, 64, 0, a->stream>>>(a->g, dt, t, a->rev);
   k_rev_slopes<<<grid, 128, 0, a->stream>>>(a->g, t, a->rev);
