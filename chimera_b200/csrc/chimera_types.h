@@ -5,7 +5,7 @@
 
 namespace chimera {
 
-constexpr int NPART = 6;  // per-tile partials: cfl speed max, |divB| max, |divB| sum, |B| max, mass, energy
+constexpr int NPART = 6;  // per-tile partials: cfl speed max, |divB| max, |divB| sum, |B|^2 max, mass, energy
 
 // Control::flags
 enum : int {

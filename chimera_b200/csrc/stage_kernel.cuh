@@ -192,10 +192,10 @@ __device__ __forceinline__ double cfl_speed(double rho, double vx, double vy, do
 
 // divB of one cell from face values (src/mhd_field_ops.f90:60-117).
 // FP32-bulk form: a cell's CFL speed c_f + |v| (FP64 pressure recovery, FP32
-// wave speeds) and |B|.  The stage-3 epilogue and the CFL kernel both use it,
+// wave speeds) and |B|^2.  The stage-3 epilogue and the CFL kernel both use it,
 // so that a dt is the same whichever of the two computed it.
 __device__ __forceinline__ void speed_f32(float M, float Mx, float My, float E, float Bx, float By,
-                                          const Member& g, double& speed, double& bmag) {
+                                          const Member& g, double& speed, double& bmag2) {
   const Prim<float> pr = get_primitive_mixed(M, Mx, My, E, Bx, By, g.gamma, g.inv_vol, float(g.inv_vol));
   const float gamma = float(g.gamma);
   const float inv_rho = 1.0f / pr.rho;
@@ -203,7 +203,7 @@ __device__ __forceinline__ void speed_f32(float M, float Mx, float My, float E, 
   float cf = sqrtf(gamma * (pr.P - 0.5f * B2) * inv_rho + B2 * inv_rho);
   if (pr.rho < 1.0e-3f) cf = fminf(cf, 50.0f);
   speed = double(cf + sqrtf(pr.vx * pr.vx + pr.vy * pr.vy));
-  bmag = double(sqrtf(B2));
+  bmag2 = double(B2);
 }
 
 __device__ __forceinline__ double divb_cell(double bx, double bxm, double by, double bym, bool has_x,
@@ -239,6 +239,9 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
   double r[6] = {sp, dmx, dsum, bmx, ms, es};
   block_reduce_partials<NT>(r, red);
   sp = r[0]; dmx = r[1]; dsum = r[2]; bmx = r[3]; ms = r[4]; es = r[5];
+  // the partials carry max |B|^2: a correctly rounded square root is monotonic,
+  // so the root of the maximum is the maximum of the roots, bit for bit
+  bmx = sqrt(bmx);
   if (threadIdx.x == 0) {
     double t = ctl->t;
     int oc = ctl->output_count;
@@ -683,7 +686,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
                                         g.inv_dx, g.inv_dy, g.square != 0));
         e_dmax = run_max(e_dmax, d);
         e_dsum += d;
-        e_bmax = run_max(e_bmax, sqrt(Bx * Bx + By * By));
+        e_bmax = run_max(e_bmax, Bx * Bx + By * By);   // |B|^2 (root taken once, at the finish)
         e_mass += double(U[0]);
         e_en += double(U[3]);
       }
@@ -755,7 +758,7 @@ __global__ void __launch_bounds__(NT) cfl_kernel(StageArgs a) {
         Prim<double> pr = get_primitive<double>(double(in[0][k]), double(in[1][k]), double(in[2][k]),
                                                 double(in[3][k]), Bx, By, g.gamma, g.vol, g.rcp_vol);
         sp = run_max(sp, cfl_speed(pr.rho, pr.vx, pr.vy, pr.P, Bx, By, g.gamma));
-        bmx = run_max(bmx, sqrt(Bx * Bx + By * By));
+        bmx = run_max(bmx, Bx * Bx + By * By);
       }
       const double d = fabs(divb_cell(bxc, bxm, byc, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
       dmx = run_max(dmx, d);

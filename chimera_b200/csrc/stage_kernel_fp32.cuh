@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
             const double dv = fabs(divb_cell(bxn, bxm, byn, bym, hx, hy, g.inv_dx, g.inv_dy, g.square != 0));
             e_dmax = run_max(e_dmax, dv);
             e_dsum += dv;
-            e_bmax = run_max(e_bmax, sqrt(Bx * Bx + By * By));
+            e_bmax = run_max(e_bmax, Bx * Bx + By * By);   // |B|^2 (root taken at the finish)
             e_mass += U[0];
             e_en += U[3];
           }
