@@ -156,6 +156,11 @@ static int cuda_fail(cudaError_t e) {
     if (_e != cudaSuccess) return cuda_fail(_e);   \
   } while (0)
 
+static bool mixed_pair(const chimera_cfg& c) {
+  return (c.bc_xlo == CHIMERA_BC_PERIODIC) != (c.bc_xhi == CHIMERA_BC_PERIODIC) ||
+         (c.bc_ylo == CHIMERA_BC_PERIODIC) != (c.bc_yhi == CHIMERA_BC_PERIODIC);
+}
+
 static int validate_cfg(const chimera_cfg* c) {
   if (!c) return CHIMERA_ERR_BAD_ARG;
   if (c->nx < 4 || c->ny < 4) return CHIMERA_ERR_BAD_ARG;                 // N >= 4 (src/mhd_init.f90:208)
@@ -164,14 +169,13 @@ static int validate_cfg(const chimera_cfg* c) {
   if (!(c->courant > 0.0) || !(c->t_out > 0.0)) return CHIMERA_ERR_BAD_ARG;
   if (!valid_bc(c->bc_xlo) || !valid_bc(c->bc_xhi) || !valid_bc(c->bc_ylo) || !valid_bc(c->bc_yhi))
     return CHIMERA_ERR_BAD_ARG;
-  // A side that wraps while its opposite side does not has no consistent
-  // ghost state; the reference accepts it but it is not supported here.
-  if ((c->bc_xlo == CHIMERA_BC_PERIODIC) != (c->bc_xhi == CHIMERA_BC_PERIODIC)) return CHIMERA_ERR_UNSUPPORTED;
-  if ((c->bc_ylo == CHIMERA_BC_PERIODIC) != (c->bc_yhi == CHIMERA_BC_PERIODIC)) return CHIMERA_ERR_UNSUPPORTED;
   if (c->riemann < 1 || c->riemann > 3) return CHIMERA_ERR_BAD_ARG;
   if (c->limiter < 1 || c->limiter > 2) return CHIMERA_ERR_BAD_ARG;
   if (c->precision != CHIMERA_FP64 && c->precision != CHIMERA_FP32_BULK && c->precision != CHIMERA_FP32_MIXED)
     return CHIMERA_ERR_BAD_ARG;
+  // A side that wraps while its opposite side does not (a mixed pair; the
+  // reference takes each side on its own, src/mhd_bc.f90:45-100): FP64 only.
+  if (mixed_pair(*c) && c->precision != CHIMERA_FP64) return CHIMERA_ERR_UNSUPPORTED;
   return CHIMERA_OK;
 }
 
@@ -451,12 +455,17 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
   h->precision = cfgs[0].precision;
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  const int nv = (h->precision == CHIMERA_FP64)       ? fp64_variant_count()
+  // a mixed pair in any member: the one tile compiled for it (FP64)
+  bool mixed = false;
+  for (int m = 0; m < n_members; ++m) mixed = mixed || mixed_pair(cfgs[m]);
+  const int nv = mixed                                 ? 1
+                 : (h->precision == CHIMERA_FP64)       ? fp64_variant_count()
                  : (h->precision == CHIMERA_FP32_BULK) ? fp32_variant_count()
                                                        : fp32m_variant_count();
   h->variants.resize(nv);
   for (int v = 0; v < nv; ++v) {
-    if (h->precision == CHIMERA_FP64) fp64_kernels(v, &h->variants[v]);
+    if (mixed) fp64_mixed_pair_kernels(&h->variants[v]);
+    else if (h->precision == CHIMERA_FP64) fp64_kernels(v, &h->variants[v]);
     else if (h->precision == CHIMERA_FP32_BULK) fp32_kernels(v, &h->variants[v]);
     else fp32m_kernels(v, &h->variants[v]);
     for (int r = 0; r < 3; ++r)
@@ -490,6 +499,8 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
     g.nx = c.nx; g.ny = c.ny;
     g.periodic_x = c.bc_xlo == CHIMERA_BC_PERIODIC;
     g.periodic_y = c.bc_ylo == CHIMERA_BC_PERIODIC;
+    g.periodic_xhi = c.bc_xhi == CHIMERA_BC_PERIODIC;
+    g.periodic_yhi = c.bc_yhi == CHIMERA_BC_PERIODIC;
     g.square = (c.dx == c.dy) ? 1 : 0;
     g.dx = c.dx; g.dy = c.dy;
     g.inv_dx = 1.0 / c.dx; g.inv_dy = 1.0 / c.dy;
@@ -816,7 +827,7 @@ int chimera_step_host(chimera_handle* h, const double* const* in, double* const*
                              cudaMemcpyDeviceToHost, h->copy_stream));
       return CHIMERA_OK;
     };
-    if (!g.periodic_y) {
+    if (!g.periodic_y && !g.periodic_yhi) {
       // a wavefront: stage 1 runs two tile rows ahead of stage 3 on the
       // handle's stream, stage 2 one row ahead on band_stream[0], stage 3 on
       // band_stream[1].  Stage 3 writes U^{n+1} over U1's rows of chunk k only
@@ -839,7 +850,7 @@ int chimera_step_host(chimera_handle* h, const double* const* in, double* const*
       // later work on the handle's stream comes after the wavefront
       CK(cudaEventRecord(h->band_join, s3));
       CK(cudaStreamWaitEvent(h->stream, h->band_join, 0));
-    } else {   // y-periodic: tile row 0 reads the last row, so stages 1 and 2 take the whole grid
+    } else {   // y wraps: tile row 0 (or the last) reads the other end, so stages 1 and 2 take the whole grid
       for (int s = 0; s < 2; ++s)
         if ((e = launch(h, ks[s], h->grid_stage[s], s + 1))) return e;
       for (int k = 0; k < nc; ++k)

@@ -27,7 +27,8 @@ struct Member {
   int nx, ny;
   int tiles_x, tiles_y;
   int tile_begin;          // first global work-list index of this member
-  int periodic_x, periodic_y;
+  int periodic_x, periodic_y;      // the low side (x = 0, y = 0) wraps
+  int periodic_xhi, periodic_yhi;  // the high side wraps (differs from the low side only in a mixed pair)
   int square;              // dx == dy: the reference's single-spacing expressions apply
   double dx, dy;
   double inv_dx, inv_dy;   // 1/dx, 1/dy as the reference computes them

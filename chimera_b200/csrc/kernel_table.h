@@ -21,6 +21,7 @@ struct KernelSet {
 // Tile-shape variants per precision (for the autotuner).
 int fp64_variant_count();
 void fp64_kernels(int variant, KernelSet* out);
+void fp64_mixed_pair_kernels(KernelSet* out);
 int fp32_variant_count();
 void fp32_kernels(int variant, KernelSet* out);
 int fp32m_variant_count();

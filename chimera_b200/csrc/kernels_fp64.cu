@@ -7,13 +7,14 @@
 namespace chimera {
 
 namespace {
-template <int TX, int TY, int NT, int MINB, bool KEEP_IN = false, bool TMA = false>
+template <int TX, int TY, int NT, int MINB, bool KEEP_IN = false, bool TMA = false, bool MIXBC = false>
 void fill(KernelSet* ks) {
   using G = TileGeom<TX, TY>;
   const int bw = TMA ? TmaBox64<TX, TY>::BW : 0, bh = TMA ? TmaBox64<TX, TY>::BH : 0;
   const size_t smem = G::template smem_bytes<double, KEEP_IN>();
 #define CHIMERA_ENTRY(S, K) \
-  ks->stage[S - 1][K - 1] = KernelEntry{(const void*)&stage_kernel<double, S, K, TX, TY, NT, MINB, KEEP_IN, TMA>, \
+  ks->stage[S - 1][K - 1] = KernelEntry{                                                                  \
+      (const void*)&stage_kernel<double, S, K, TX, TY, NT, MINB, KEEP_IN, TMA, UNIT_FP64, MIXBC>,          \
                                         smem, TX, TY, NT, bw, bh}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
@@ -39,5 +40,8 @@ void fp64_kernels(int variant, KernelSet* out) {
     default: fill<32, 16, 256, 2, false, true>(out); break;   // phase 1 from TMA boxes (interior tiles)
   }
 }
+
+// The one tile for grids with a periodic side facing a non-periodic one.
+void fp64_mixed_pair_kernels(KernelSet* out) { fill<32, 16, 256, 2, false, false, true>(out); }
 
 }  // namespace chimera

@@ -140,6 +140,8 @@ extern "C" int chimera_rk3_step_noalloc(const chimera_cfg* cfg, double* Mass, do
   g.tile_begin = 0;
   g.periodic_x = cfg->bc_xlo == CHIMERA_BC_PERIODIC;
   g.periodic_y = cfg->bc_ylo == CHIMERA_BC_PERIODIC;
+  g.periodic_xhi = g.periodic_x;   // (pairs alike: checked above)
+  g.periodic_yhi = g.periodic_y;
   g.square = (cfg->dx == cfg->dy) ? 1 : 0;
   g.dx = cfg->dx; g.dy = cfg->dy;
   g.inv_dx = 1.0 / cfg->dx; g.inv_dy = 1.0 / cfg->dy;

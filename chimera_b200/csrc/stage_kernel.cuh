@@ -48,11 +48,13 @@ __device__ __forceinline__ void* load_ptr(void* const* p) {
 }
 
 // Source cell of a (possibly out-of-domain) tile position: periodic wrap or
-// the nearest cell.  Positions of a ragged last tile can lie more than one
-// period beyond a small grid, so the wrap is a true modulo.
-__device__ __forceinline__ int map_index(int g, int n, int periodic) {
+// the nearest cell, by the rule of the side it lies beyond (plo below 0, phi
+// at n and above; src/mhd_bc.f90:36-121 takes each side on its own).
+// Positions of a ragged last tile can lie more than one period beyond a small
+// grid, so the wrap is a true modulo.
+__device__ __forceinline__ int map_index(int g, int n, int plo, int phi) {
   if (g >= 0 && g < n) return g;
-  if (periodic) {
+  if (g < 0 ? plo : phi) {
     // g mod n by whole periods: one step for every grid of at least a tile's
     // width, a few for tiny ones -- no integer division on the common path
     while (g < 0) g += n;
@@ -124,7 +126,7 @@ __device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_nex
       const int q = it / (ROWS * LPR), rem = it % (ROWS * LPR);
       const int r = rem / LPR, l = rem % LPR;
       const char* row = reinterpret_cast<const char*>(g.buf[in_buf][q]) +
-                        size_t(map_index(j0 - 3 + r, ny, g.periodic_y)) * nx * sizeof(R);
+                        size_t(map_index(j0 - 3 + r, ny, g.periodic_y, g.periodic_yhi)) * nx * sizeof(R);
       touch(row + size_t(c0) * sizeof(R), row + size_t(c1) * sizeof(R), l);
     }
   }
@@ -135,7 +137,7 @@ __device__ __forceinline__ void prefetch_next_tile(const StageArgs& a, int w_nex
       const int q = it / (ROWS0 * LPR), rem = it % (ROWS0 * LPR);
       const int r = rem / LPR, l = rem % LPR;
       const char* row = reinterpret_cast<const char*>(g.buf[sbuf][q]) +
-                        size_t(map_index(j0 - 1 + r, ny, g.periodic_y)) * nx * sizeof(R);
+                        size_t(map_index(j0 - 1 + r, ny, g.periodic_y, g.periodic_yhi)) * nx * sizeof(R);
       touch(row + size_t(c0) * sizeof(R), row + size_t(c1) * sizeof(R), l);
     }
   }
@@ -295,9 +297,15 @@ __device__ void member_finish(const Member& g, Control* ctl, const double* part,
 // anyway, keeps the four conserved fields of the tile's own cells in shared
 // memory, and phase 3b reads them there instead of from L2 (16 KB more for a
 // 32 x 16 tile; fewer live registers through the update, and fewer spills).
+// MIXBC: a periodic side may face a non-periodic one (a mixed pair).  A halo
+// cell that wraps across such a pair must see its neighbours as the cell it
+// copies does (its neighbour across the non-periodic side is itself), and the
+// face and corner values computed in the halo must be the ones the owning
+// tile computes; the checks cost instructions on every face, so grids without
+// a mixed pair run the MIXBC = false instantiations.
 // ----------------------------------------------------------------------------
 template <typename R, int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool KEEP_IN = false,
-          bool TMA = false, int UNIT = UNIT_FP64>
+          bool TMA = false, int UNIT = UNIT_FP64, bool MIXBC = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
   using G = TileGeom<TX, TY>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -335,7 +343,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     Control* ctl = a.ctl + m;
     if (ctl->active == 0) continue;  // uniform across the CTA
     const int nx = g.nx, ny = g.ny;
-    const int px = g.periodic_x, py = g.periodic_y;
+    const int px = g.periodic_x, py = g.periodic_y;                   // low sides
+    const int pxh = MIXBC ? g.periodic_xhi : px, pyh = MIXBC ? g.periodic_yhi : py;   // high sides
     const int lt = w - g.tile_begin;
     const int i0 = (lt % g.tiles_x) * TX;
     const int j0 = (lt / g.tiles_x) * TY;
@@ -420,8 +429,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
       for (int q = 0; q < 6; ++q) in[q] = reinterpret_cast<const R*>(g.buf[in_buf][q]);
       for (int p = tid; p < G::NP; p += NT) {
         const int qx = p % G::PX, qy = p / G::PX;
-        const int si = map_index(i0 - 2 + qx, nx, px);
-        const int sj = map_index(j0 - 2 + qy, ny, py);
+        const int si = map_index(i0 - 2 + qx, nx, px, pxh);
+        const int sj = map_index(j0 - 2 + qy, ny, py, pyh);
         const size_t idx = size_t(sj) * nx + si;
         const R bxc = in[4][idx];
         const R byc = in[5][idx];
@@ -467,23 +476,39 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
       const R hh = R(ydir ? g.hy : g.hx);             // 0.5 * spacing
       R L[6], Rv[6];
       bool reset = false;
+      // mixed pairs: the low cell's neighbours that are its own ghost (a cell
+      // wrapped across a pair, next to the non-periodic side), and a high cell
+      // wrapped from the far side whose low neighbour is its own ghost
+      bool own_xp = false, own_xm = false, own_yp = false, own_ym = false, own_bm = false;
+      if constexpr (MIXBC) {
+        const int gax = i0 + li - 1, gay = j0 + lj - 1;   // the low cell
+        own_xp = px && !pxh && gax == -1;
+        own_xm = !px && pxh && gax == nx;
+        own_yp = py && !pyh && gay == -1;
+        own_ym = !py && pyh && gay == ny;
+        own_bm = ydir ? (!py && pyh && gay + 1 == ny) : (!px && pxh && gax + 1 == nx);
+      }
+      const bool own_np = ydir ? own_yp : own_xp;   // the high cell is the low cell's own ghost
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         const R* s = sP + q * G::NP;
-        const R fm = s[pa - on], f0 = s[pa], fp = s[pa + on], fpp = s[pa + 2 * on];
+        const R fm = s[pa - on], f0 = s[pa];
+        R fp = s[pa + on], fpp = s[pa + 2 * on];
+        if (MIXBC && own_np) { fp = f0; fpp = f0; }
+        const R fb0 = (MIXBC && own_bm) ? fp : f0;    // the high cell's low neighbour
         // apply_slope_limiter (src/mhd_derivatives.f90:50-127) or compute_gradients (:15-47)
         R sa, sb;
         if (slope_on) {
           if (van_leer) {
             sa = limit_slope<R, LIMITER_VAN_LEER>((f0 - fm) * inv_h, (fp - f0) * inv_h);
-            sb = limit_slope<R, LIMITER_VAN_LEER>((fp - f0) * inv_h, (fpp - fp) * inv_h);
+            sb = limit_slope<R, LIMITER_VAN_LEER>((fp - fb0) * inv_h, (fpp - fp) * inv_h);
           } else {
             sa = limit_slope<R, LIMITER_MC>((f0 - fm) * inv_h, (fp - f0) * inv_h);
-            sb = limit_slope<R, LIMITER_MC>((fp - f0) * inv_h, (fpp - fp) * inv_h);
+            sb = limit_slope<R, LIMITER_MC>((fp - fb0) * inv_h, (fpp - fp) * inv_h);
           }
         } else {
           sa = (fp - fm) * inv_2h;
-          sb = (fpp - f0) * inv_2h;
+          sb = (fpp - fb0) * inv_2h;
         }
         // reconstruction (src/mhd_derivatives.f90:160-182): left state from the low
         // cell, right state = the high cell extrapolated back (temp_x(i+1)).
@@ -494,8 +519,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
           // MOOD bounds of the LOW cell (:190-216), applied to both states and
           // resetting both to the low cell's value (the reference's XR/YR rule).
           // (the bounds only feed comparisons: hardware min / max)
-          R lo = hmin(hmin(hmin(hmin(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
-          const R hi = hmax(hmax(hmax(hmax(f0, s[pa + 1]), s[pa - 1]), s[pa + G::PX]), s[pa - G::PX]);
+          R nxp = s[pa + 1], nxm = s[pa - 1], nyp = s[pa + G::PX], nym = s[pa - G::PX];
+          if (MIXBC && own_xp) nxp = f0;
+          if (MIXBC && own_xm) nxm = f0;
+          if (MIXBC && own_yp) nyp = f0;
+          if (MIXBC && own_ym) nym = f0;
+          R lo = hmin(hmin(hmin(hmin(f0, nxp), nxm), nyp), nym);
+          const R hi = hmax(hmax(hmax(hmax(f0, nxp), nxm), nyp), nym);
           if (rp) lo = hmax(R(0.1e-8), lo);
           if (vL < lo || vL > hi) { vL = f0; reset = true; }
           if (vR < lo || vR > hi) { vR = f0; reset = true; }
@@ -558,10 +588,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     auto Ez = [&](int ci, int cj) -> R {
       const int xi = (cj - j0 + 1) * G::FXW + (ci - i0 + 1);
       const R fa = FByX[xi];
-      const R up = (cj == ny - 1 && !py) ? fa : FByX[xi + G::FXW];
+      // zero gradient past a non-periodic high side -- also for the corner row
+      // below y = 0 that wraps to it (mixed pair)
+      const bool up_own = (cj == ny - 1 && !pyh) || (MIXBC && cj == -1 && py && !pyh);
+      const R up = up_own ? fa : FByX[xi + G::FXW];
       const int yi = (cj - j0 + 1) * G::FYW + (ci - i0 + 1);
       const R fb = FBxY[yi];
-      const R right = (ci == nx - 1 && !px) ? fb : FBxY[yi + 1];
+      const bool right_own = (ci == nx - 1 && !pxh) || (MIXBC && ci == -1 && px && !pxh);
+      const R right = right_own ? fb : FBxY[yi + 1];
       return R(0.25) * (((-fa - up) + fb) + right);
     };
     const R inv_dx = R(g.inv_dx), inv_dy = R(g.inv_dy);

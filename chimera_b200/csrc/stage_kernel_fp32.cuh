@@ -313,8 +313,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       for (int q = 0; q < 6; ++q) src[q] = reinterpret_cast<const S*>(g.buf[in_buf][q]);
       for (int p = tid; p < G::NP; p += NT) {
         const int qx = p % G::PX, qy = p / G::PX;
-        const int si = map_index(i0 - 2 + qx, nx, px);
-        const int sj = map_index(j0 - 2 + qy, ny, py);
+        const int si = map_index(i0 - 2 + qx, nx, px, px);
+        const int sj = map_index(j0 - 2 + qy, ny, py, py);
         const size_t idx = size_t(sj) * nx + si;
         const double bxc = src[4][idx], byc = src[5][idx];
         double Bx, By;
@@ -340,8 +340,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const int p = tid + k * NT;
         if (p < G::NP) {
           const int qx = p % G::PX, qy = p / G::PX;
-          const int si = map_index(i0 - 2 + qx, nx, px);
-          const int sj = map_index(j0 - 2 + qy, ny, py);
+          const int si = map_index(i0 - 2 + qx, nx, px, px);
+          const int sj = map_index(j0 - 2 + qy, ny, py, py);
           const size_t idx = size_t(sj) * nx + si;
           const size_t ixm = (si > 0) ? idx - 1 : (px ? idx + (nx - 1) : idx);
           const size_t iym = (sj > 0) ? idx - nx : (py ? idx + size_t(ny - 1) * nx : idx);
@@ -354,8 +354,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const int p = tid + k * NT;
         if (p < G::NP) {
           const int qx = p % G::PX, qy = p / G::PX;
-          const int si = map_index(i0 - 2 + qx, nx, px);
-          const int sj = map_index(j0 - 2 + qy, ny, py);
+          const int si = map_index(i0 - 2 + qx, nx, px, px);
+          const int sj = map_index(j0 - 2 + qy, ny, py, py);
           const S Bx = (si > 0 || px) ? S(0.5) * (ld[k][4] + ld[k][5]) : ld[k][4];
           const S By = (sj > 0 || py) ? S(0.5) * (ld[k][6] + ld[k][7]) : ld[k][6];
           const Prim<R> pr = get_primitive_mixed(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, g.gamma,

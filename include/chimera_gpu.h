@@ -95,7 +95,10 @@ typedef struct chimera_handle chimera_handle;
 /* ---- single grid --------------------------------------------------------- */
 
 /* Create a solver for one grid.  stream: a cudaStream_t, or NULL to create one.
- * Replaces the allocations of src/mhd_init.f90:99-164 for the path's arrays. */
+ * Each side takes its own boundary flag, as src/mhd_bc.f90:45-100 does; a
+ * periodic side facing a non-periodic one is FP64 only (CHIMERA_ERR_UNSUPPORTED
+ * for the FP32 forms).  Replaces the allocations of src/mhd_init.f90:99-164 for
+ * the path's arrays. */
 int chimera_create(const chimera_cfg* cfg, void* stream, chimera_handle** out);
 
 /* Copy a conserved state in (host or device arrays); marks dt stale.  Host
@@ -253,9 +256,9 @@ int chimera_set_dt_device(chimera_handle* h, const double* d_dt);
  * thermal-check decisions are the forward's, and at a kink the derivative is
  * that of the branch the forward took.  Pointer arguments are arrays of six
  * device pointers (Mass, Momx, Momy, Energy, b_x, b_y), each a dense (nx, ny)
- * array.  Boundaries as for chimera_create: every non-periodic kind acts as
- * outflow, and a periodic side paired with a non-periodic opposite side is
- * CHIMERA_ERR_UNSUPPORTED.  All calls synchronise the adjoint's stream. */
+ * array.  Boundaries: every non-periodic kind acts as outflow; a periodic
+ * side facing a non-periodic one is CHIMERA_ERR_UNSUPPORTED here (the FP64
+ * handles accept it).  All calls synchronise the adjoint's stream. */
 typedef struct chimera_adjoint chimera_adjoint;
 int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chimera_adjoint** out);
 int chimera_adjoint_step(chimera_adjoint* a, const double* const* U_n, double dt,
@@ -288,6 +291,8 @@ void chimera_adjoint_destroy(chimera_adjoint* a);
  *     untouched (as chimera_step leaves an inactive state).
  *   - stream (null = the current device's legacy stream) must belong to the
  *     current device, whose scratch the call uses; CHIMERA_ERR_BAD_ARG if not.
+ *   - FP64 only, and each pair of opposite sides alike (a periodic side facing
+ *     a non-periodic one: CHIMERA_ERR_UNSUPPORTED; chimera_create takes it).
  *   - The first call on a device looks up the scratch's device address; make
  *     that first call before any stream capture.
  *   - Every call shares the one scratch array of its device, which keeps the
