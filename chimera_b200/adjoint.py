@@ -11,7 +11,7 @@ function of the state, so the derivative of the CFL reduction is not taken;
 obtain the dt sequence from a primal run (``cfl_dts``) and reuse it.  The MOOD,
 floor and thermal-check decisions and the limiter branches are the forward's;
 at a kink the derivative is that of the branch the forward took (one-sided).
-Periodic or outflow sides (each pair of opposite sides alike).
+Periodic or outflow sides, each side on its own.
 
 Forward precision: FP64 (the tape kernels, bit-identical to the fused FP64
 step) or a reduced form -- ``FP32_BULK`` or ``FP32_MIXED`` -- in which the
@@ -57,7 +57,7 @@ def _ptr6(ts):
 
 
 class Adjoint:
-    """Handle for the adjoint kernels of one grid (FP64; periodic or outflow sides)."""
+    """Handle for the adjoint kernels of one grid (FP64; periodic or outflow sides, each on its own)."""
 
     def __init__(self, cfg: SolverConfig):
         self.cfg = cfg.replace(precision=FP64)

@@ -28,8 +28,9 @@
 // with forward-mode dual numbers (dual.cuh): at a kink (limiter branch, min /
 // max, floor) the derivative is that of the branch the forward took.
 //
-// Boundary conditions: periodic or outflow (zero-gradient ghost cells) in x
-// and in y, each pair of opposite sides alike.  At an outflow side the forward
+// Boundary conditions: periodic or outflow (zero-gradient ghost cells), each
+// side on its own -- a periodic side may face an outflow one, whose faces and
+// ghosts then follow the rules of the side they lie beyond.  At an outflow side the forward
 // takes the nearest cell for every ghost position (src/mhd_bc.f90:36-121), the
 // outflow face->cell B (src/mhd_field_ops.f90:120-156), curl copy
 // (src/mhd_flux.f90:79-136), update without the incoming face
@@ -54,14 +55,17 @@ struct AdjGeom {
   int nx, ny;
   double dx, dy, inv_dx, inv_dy, inv_2dx, inv_2dy, hx, hy, gamma, vol;
   int riemann, limiter, slope, mood;
-  int px, py;   // periodic in x / y (else outflow)
+  int px, py;     // the low side (x = 0 / y = 0) is periodic (else outflow)
+  int pxh, pyh;   // the high side is periodic (differs from the low side in a mixed pair)
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 // the cell a ghost position i (one or two cells beyond the grid) takes its
-// value from: periodic wrap, or the nearest cell (outflow)
-__device__ __forceinline__ int src(int i, int n, int periodic) {
-  return periodic ? wrap(i, n) : (i < 0 ? 0 : (i >= n ? n - 1 : i));
+// value from, by the rule of the side it lies beyond (plo below 0, phi at n
+// and above): periodic wrap, or the nearest cell (outflow)
+__device__ __forceinline__ int src(int i, int n, int plo, int phi) {
+  if (i >= 0 && i < n) return i;
+  return (i < 0 ? plo : phi) ? wrap(i, n) : (i < 0 ? 0 : n - 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -94,8 +98,8 @@ __global__ void k_tape_prims(AdjGeom g, const double* const* __restrict__ U, Sta
 // decision flags; the same operations as phase 2 of stage_kernel.
 template <typename R>
 __device__ __forceinline__ void face_states(const AdjGeom& g, const StageTape& t, int a, int b, int am, int bp,
-                                            int ax_p, int ax_m, int ay_p, int ay_m, bool ydir, R* L, R* Rv,
-                                            uint32_t* flags) {
+                                            int ax_p, int ax_m, int ay_p, int ay_m, bool ydir, bool b_own, R* L,
+                                            R* Rv, uint32_t* flags) {
   const double inv_h = ydir ? g.inv_dy : g.inv_dx;
   const double inv_2h = ydir ? g.inv_2dy : g.inv_2dx;
   const double hh = ydir ? g.hy : g.hx;
@@ -103,18 +107,19 @@ __device__ __forceinline__ void face_states(const AdjGeom& g, const StageTape& t
   for (int q = 0; q < 6; ++q) {
     const double* s = t.P[q];
     const double fm = s[am], f0 = s[a], fp = s[b], fpp = s[bp];
+    const double fb0 = b_own ? fp : f0;   // the high cell's low neighbour in its slope
     double sa, sb;
     if (g.slope) {
       if (g.limiter == LIMITER_VAN_LEER) {
         sa = limit_slope<double, LIMITER_VAN_LEER>((f0 - fm) * inv_h, (fp - f0) * inv_h);
-        sb = limit_slope<double, LIMITER_VAN_LEER>((fp - f0) * inv_h, (fpp - fp) * inv_h);
+        sb = limit_slope<double, LIMITER_VAN_LEER>((fp - fb0) * inv_h, (fpp - fp) * inv_h);
       } else {
         sa = limit_slope<double, LIMITER_MC>((f0 - fm) * inv_h, (fp - f0) * inv_h);
-        sb = limit_slope<double, LIMITER_MC>((fp - f0) * inv_h, (fpp - fp) * inv_h);
+        sb = limit_slope<double, LIMITER_MC>((fp - fb0) * inv_h, (fpp - fp) * inv_h);
       }
     } else {
       sa = (fp - fm) * inv_2h;
-      sb = (fpp - f0) * inv_2h;
+      sb = (fpp - fb0) * inv_2h;
     }
     double vL = f0 + hh * sa;
     double vR = fp - hh * sb;
@@ -149,27 +154,35 @@ __device__ __forceinline__ void face_states(const AdjGeom& g, const StageTape& t
 // neighbour indices for the face with low cell (i, j) in direction ydir
 struct FaceIdx {
   int a, b, am, bp, axp, axm, ayp, aym;
-  bool b_real;   // the high cell is a cell of the grid (not the ghost past an outflow side)
+  int to;       // the cell above the face, whose update takes the face's flux if b_in
+  bool b_in;    // the flux enters that cell (not past an outflow high side, nor into an
+                // outflow low side's first cell through a wrap)
+  bool b_own;   // mixed pair, outflow low / periodic high side: the high cell is cell 0
+                // through the wrap, and its slope's low neighbour is its own ghost
 };
 __device__ __forceinline__ FaceIdx face_idx(const AdjGeom& g, int i, int j, bool ydir) {
   FaceIdx f;
   const int nx = g.nx, ny = g.ny;
   f.a = j * nx + i;
   if (!ydir) {
-    f.b = j * nx + src(i + 1, nx, g.px);
-    f.am = j * nx + src(i - 1, nx, g.px);
-    f.bp = j * nx + src(i + 2, nx, g.px);
-    f.b_real = g.px || i + 1 < nx;
+    f.b = j * nx + src(i + 1, nx, g.px, g.pxh);
+    f.am = j * nx + src(i - 1, nx, g.px, g.pxh);
+    f.bp = j * nx + src(i + 2, nx, g.px, g.pxh);
+    f.to = j * nx + wrap(i + 1, nx);
+    f.b_in = i + 1 < nx || g.px;
+    f.b_own = !g.px && g.pxh && i == nx - 1;
   } else {
-    f.b = src(j + 1, ny, g.py) * nx + i;
-    f.am = src(j - 1, ny, g.py) * nx + i;
-    f.bp = src(j + 2, ny, g.py) * nx + i;
-    f.b_real = g.py || j + 1 < ny;
+    f.b = src(j + 1, ny, g.py, g.pyh) * nx + i;
+    f.am = src(j - 1, ny, g.py, g.pyh) * nx + i;
+    f.bp = src(j + 2, ny, g.py, g.pyh) * nx + i;
+    f.to = wrap(j + 1, ny) * nx + i;
+    f.b_in = j + 1 < ny || g.py;
+    f.b_own = !g.py && g.pyh && j == ny - 1;
   }
-  f.axp = j * nx + src(i + 1, nx, g.px);
-  f.axm = j * nx + src(i - 1, nx, g.px);
-  f.ayp = src(j + 1, ny, g.py) * nx + i;
-  f.aym = src(j - 1, ny, g.py) * nx + i;
+  f.axp = j * nx + src(i + 1, nx, g.px, g.pxh);
+  f.axm = j * nx + src(i - 1, nx, g.px, g.pxh);
+  f.ayp = src(j + 1, ny, g.py, g.pyh) * nx + i;
+  f.aym = src(j - 1, ny, g.py, g.pyh) * nx + i;
   return f;
 }
 
@@ -183,7 +196,7 @@ __global__ void k_tape_faces(AdjGeom g, StageTape t) {
     const FaceIdx f = face_idx(g, i, j, ydir);
     double L[6], Rv[6];
     uint32_t fl;
-    face_states<double>(g, t, f.a, f.b, f.am, f.bp, f.axp, f.axm, f.ayp, f.aym, ydir, L, Rv, &fl);
+    face_states<double>(g, t, f.a, f.b, f.am, f.bp, f.axp, f.axm, f.ayp, f.aym, ydir, f.b_own, L, Rv, &fl);
     const double unL = ydir ? L[2] : L[1], unR = ydir ? Rv[2] : Rv[1];
     const double utL = ydir ? L[1] : L[2], utR = ydir ? Rv[1] : Rv[2];
     const double bnL = ydir ? L[5] : L[4], bnR = ydir ? Rv[5] : Rv[4];
@@ -204,9 +217,9 @@ __device__ __forceinline__ double Ez_at(const AdjGeom& g, const StageTape& t, in
   i = wrap(i, nx);
   j = wrap(j, ny);
   const double fa = t.Fx[4][j * nx + i];
-  const double up = (j == ny - 1 && !g.py) ? fa : t.Fx[4][wrap(j + 1, ny) * nx + i];   // outflow: zero gradient
+  const double up = (j == ny - 1 && !g.pyh) ? fa : t.Fx[4][wrap(j + 1, ny) * nx + i];   // outflow: zero gradient
   const double fb = t.Fy[4][j * nx + i];
-  const double right = (i == nx - 1 && !g.px) ? fb : t.Fy[4][j * nx + wrap(i + 1, nx)];
+  const double right = (i == nx - 1 && !g.pxh) ? fb : t.Fy[4][j * nx + wrap(i + 1, nx)];
   return 0.25 * (((-fa - up) + fb) + right);
 }
 
@@ -412,23 +425,23 @@ __global__ void k_rev_faces(AdjGeom g, double dt, StageTape t, RevBuf r) {
     double lF[5];
     const double wgt = ydir ? ay : ax;
     // the flux leaves cell a and enters cell b (none past an outflow high side)
-    for (int q = 0; q < 4; ++q) lF[q] = wgt * ((f.b_real ? r.lUp[q][f.b] : 0.0) - r.lUp[q][c]);
+    for (int q = 0; q < 4; ++q) lF[q] = wgt * ((f.b_in ? r.lUp[q][f.to] : 0.0) - r.lUp[q][c]);
     // Ez(i,j) = 1/4 (-Fx(i,j) - Fx(i,j+1) + Fy(i,j) + Fy(i+1,j)); at an outflow
     // high side Fx(i,ny) / Fy(nx,j) is the face itself (zero gradient)
     const double e0 = r.lEz[c];
     if (!ydir) {
-      double s4 = (j > 0 || g.py) ? e0 + r.lEz[wrap(j - 1, g.ny) * g.nx + i] : e0;
-      if (j == g.ny - 1 && !g.py) s4 += e0;
+      double s4 = (j > 0 || g.pyh) ? e0 + r.lEz[wrap(j - 1, g.ny) * g.nx + i] : e0;
+      if (j == g.ny - 1 && !g.pyh) s4 += e0;
       lF[4] = -0.25 * s4;
     } else {
-      double s4 = (i > 0 || g.px) ? e0 + r.lEz[j * g.nx + wrap(i - 1, g.nx)] : e0;
-      if (i == g.nx - 1 && !g.px) s4 += e0;
+      double s4 = (i > 0 || g.pxh) ? e0 + r.lEz[j * g.nx + wrap(i - 1, g.nx)] : e0;
+      if (i == g.nx - 1 && !g.pxh) s4 += e0;
       lF[4] = 0.25 * s4;
     }
     // recompute the face states (values + flags), then the flux Jacobian
     double L[6], Rv[6];
     uint32_t fl;
-    face_states<double>(g, t, f.a, f.b, f.am, f.bp, f.axp, f.axm, f.ayp, f.aym, ydir, L, Rv, &fl);
+    face_states<double>(g, t, f.a, f.b, f.am, f.bp, f.axp, f.axm, f.ayp, f.aym, ydir, f.b_own, L, Rv, &fl);
     // solver inputs in (normal, tangential) order, seeded 0..11
     const int perm[6] = {0, ydir ? 2 : 1, ydir ? 1 : 2, 3, ydir ? 5 : 4, ydir ? 4 : 5};  // input slot -> field
     D in[12];
@@ -483,23 +496,26 @@ __global__ void k_rev_slopes(AdjGeom g, StageTape t, RevBuf r) {
   const int n = g.nx * g.ny;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int i = c % g.nx, j = c / g.nx;
-    const int cxm = j * g.nx + src(i - 1, g.nx, g.px), cym = src(j - 1, g.ny, g.py) * g.nx + i;
-    const int cxp = j * g.nx + src(i + 1, g.nx, g.px), cyp = src(j + 1, g.ny, g.py) * g.nx + i;
-    // at an outflow low side there is no face below the cell; past an outflow
-    // high side the ghost's value is this cell's (its slope, from two equal
-    // differences, depends on no cell)
-    const bool hx = i > 0 || g.px, hy = j > 0 || g.py;
-    const bool ex = !g.px && i == g.nx - 1, ey = !g.py && j == g.ny - 1;
+    // the slope stencil of this cell (each side's ghost rule)
+    const int cxm = j * g.nx + src(i - 1, g.nx, g.px, g.pxh), cym = src(j - 1, g.ny, g.py, g.pyh) * g.nx + i;
+    const int cxp = j * g.nx + src(i + 1, g.nx, g.px, g.pxh), cyp = src(j + 1, g.ny, g.py, g.pyh) * g.nx + i;
+    // the face below this cell, whose high cell it is: none at x = 0 / y = 0
+    // unless the high side wraps to it; past an outflow high side the ghost's
+    // value is this cell's (its slope, from two equal differences, depends on
+    // no cell)
+    const int fxm = j * g.nx + wrap(i - 1, g.nx), fym = wrap(j - 1, g.ny) * g.nx + i;
+    const bool hx = i > 0 || g.pxh, hy = j > 0 || g.pyh;
+    const bool ex = !g.pxh && i == g.nx - 1, ey = !g.pyh && j == g.ny - 1;
     for (int q = 0; q < 6; ++q) {
       // this cell is the low cell of faces (c, x) and (c, y), the high cell of (cxm, x) and (cym, y)
-      double lv = r.fX[4 * q + 0][c] + r.fY[4 * q + 0][c] + (hx ? r.fX[4 * q + 2][cxm] : 0.0) +
-                  (hy ? r.fY[4 * q + 2][cym] : 0.0);
+      double lv = r.fX[4 * q + 0][c] + r.fY[4 * q + 0][c] + (hx ? r.fX[4 * q + 2][fxm] : 0.0) +
+                  (hy ? r.fY[4 * q + 2][fym] : 0.0);
       if (ex) lv += r.fX[4 * q + 2][c];
       if (ey) lv += r.fY[4 * q + 2][c];
       r.lPc[q][c] = lv;
       for (int d = 0; d < 2; ++d) {
-        const double ls = (d == 0) ? (r.fX[4 * q + 1][c] + (hx ? r.fX[4 * q + 3][cxm] : 0.0))
-                                   : (r.fY[4 * q + 1][c] + (hy ? r.fY[4 * q + 3][cym] : 0.0));
+        const double ls = (d == 0) ? (r.fX[4 * q + 1][c] + (hx ? r.fX[4 * q + 3][fxm] : 0.0))
+                                   : (r.fY[4 * q + 1][c] + (hy ? r.fY[4 * q + 3][fym] : 0.0));
         const double fm = t.P[q][d == 0 ? cxm : cym], f0 = t.P[q][c], fp = t.P[q][d == 0 ? cxp : cyp];
         const double inv_h = d == 0 ? g.inv_dx : g.inv_dy;
         double wl, wr;
@@ -548,12 +564,28 @@ __global__ void k_rev_prims(AdjGeom g, StageTape t, RevBuf r, const double* cons
       for (int d = 0; d < 2; ++d) {
         const double* w0 = r.w[(q * 2 + d) * 2 + 0];
         const double* w1 = r.w[(q * 2 + d) * 2 + 1];
-        const bool per = d == 0 ? g.px : g.py;
+        const bool per = d == 0 ? g.px : g.py, perh = d == 0 ? g.pxh : g.pyh;
         const int k = d == 0 ? i : j, nk = d == 0 ? g.nx : g.ny;
         const int cm = d == 0 ? cxm : cym, cp = d == 0 ? cxp : cyp;
-        if (per || (k > 0 && k < nk - 1)) v += w0[c] - w1[c] - w0[cp] + w1[cm];
-        else if (k == 0) v += (-w1[c]) - w0[cp];
-        else v += w0[c] + w1[cm];
+        if (per != perh) {
+          // a mixed pair: this cell's own slope, with its own ghost below / above
+          // where that side is outflow, then the slopes of the cells whose low /
+          // high neighbour it is (across a periodic side, through the wrap)
+          const int wm = d == 0 ? j * g.nx + wrap(i - 1, g.nx) : wrap(j - 1, g.ny) * g.nx + i;
+          const int wp = d == 0 ? j * g.nx + wrap(i + 1, g.nx) : wrap(j + 1, g.ny) * g.nx + i;
+          double own = w0[c] - w1[c];
+          if (k == 0 && !per) own -= w0[c];
+          if (k == nk - 1 && !perh) own += w1[c];
+          v += own;
+          if (k + 1 < nk || per) v -= w0[wp];
+          if (k > 0 || perh) v += w1[wm];
+        } else if (per || (k > 0 && k < nk - 1)) {
+          v += w0[c] - w1[c] - w0[cp] + w1[cm];
+        } else if (k == 0) {
+          v += (-w1[c]) - w0[cp];
+        } else {
+          v += w0[c] + w1[cm];
+        }
       }
       lP[q] = v;
     }
@@ -642,12 +674,8 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
   if (cfg->riemann < 1 || cfg->riemann > 3 || cfg->limiter < 1 || cfg->limiter > 2) return CHIMERA_ERR_BAD_ARG;
   for (int b : {cfg->bc_xlo, cfg->bc_xhi, cfg->bc_ylo, cfg->bc_yhi})
     if (b < CHIMERA_BC_PERIODIC || b > CHIMERA_BC_INFLOW) return CHIMERA_ERR_BAD_ARG;
-  // every non-periodic kind acts as outflow (src/mhd_bc.f90:36-121); a side
-  // that wraps while its opposite side does not is not supported (as for the
-  // forward handles)
-  if ((cfg->bc_xlo == CHIMERA_BC_PERIODIC) != (cfg->bc_xhi == CHIMERA_BC_PERIODIC) ||
-      (cfg->bc_ylo == CHIMERA_BC_PERIODIC) != (cfg->bc_yhi == CHIMERA_BC_PERIODIC))
-    return CHIMERA_ERR_UNSUPPORTED;
+  // every non-periodic kind acts as outflow (src/mhd_bc.f90:36-121), each
+  // side on its own (a periodic side may face an outflow one)
   if (cfg->precision != CHIMERA_FP64) return CHIMERA_ERR_UNSUPPORTED;
   if ((long long)cfg->nx * cfg->ny >= (1LL << 31)) return CHIMERA_ERR_TOO_LARGE;   // int cell indices
   chimera_adjoint* a = new (std::nothrow) chimera_adjoint();
@@ -665,6 +693,8 @@ extern "C" int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chim
   g.mood = cfg->mood ? 1 : 0;
   g.px = cfg->bc_xlo == CHIMERA_BC_PERIODIC;
   g.py = cfg->bc_ylo == CHIMERA_BC_PERIODIC;
+  g.pxh = cfg->bc_xhi == CHIMERA_BC_PERIODIC;
+  g.pyh = cfg->bc_yhi == CHIMERA_BC_PERIODIC;
   a->n = cfg->nx * cfg->ny;
   if (stream) a->stream = (cudaStream_t)stream;
   else {

@@ -250,15 +250,15 @@ int chimera_get_dt_device(chimera_handle* h, double* d_dt);
 /* Set every member's dt from d_dt[member] (device memory) for the next step. */
 int chimera_set_dt_device(chimera_handle* h, const double* d_dt);
 
-/* ---- discrete adjoint of one RK3 step (FP64, periodic or outflow sides) --------
+/* ---- discrete adjoint of one RK3 step (FP64, periodic or outflow sides) ----
  * No counterpart in the reference.  lambda_n = (dU_{n+1}/dU_n)^T lambda_{n+1}
  * for the step U_n -> U_{n+1} with a given (frozen) dt: the MOOD, floor and
  * thermal-check decisions are the forward's, and at a kink the derivative is
  * that of the branch the forward took.  Pointer arguments are arrays of six
  * device pointers (Mass, Momx, Momy, Energy, b_x, b_y), each a dense (nx, ny)
- * array.  Boundaries: every non-periodic kind acts as outflow; a periodic
- * side facing a non-periodic one is CHIMERA_ERR_UNSUPPORTED here (the FP64
- * handles accept it).  All calls synchronise the adjoint's stream. */
+ * array.  Boundaries: every non-periodic kind acts as outflow, each side on
+ * its own (a periodic side may face a non-periodic one).  All calls
+ * synchronise the adjoint's stream. */
 typedef struct chimera_adjoint chimera_adjoint;
 int chimera_adjoint_create(const chimera_cfg* cfg, void* stream, chimera_adjoint** out);
 int chimera_adjoint_step(chimera_adjoint* a, const double* const* U_n, double dt,

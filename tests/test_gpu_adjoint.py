@@ -47,7 +47,8 @@ def _loss_gpu(A, adj, cfg, prims, dts, K, precision=FP64):
     return A.magnetic_energy(cfg, UN)
 
 
-@pytest.mark.parametrize("case", ["field_loop_hlle_vl", "ot_rusanov_mc", "rotor_outflow", "generic_mixed_hlld"])
+@pytest.mark.parametrize("case", ["field_loop_hlle_vl", "ot_rusanov_mc", "rotor_outflow", "generic_mixed_hlld",
+                                  "generic_pairs_hlld"])
 def test_tape_forward_is_the_fused_step(A, case):
     from chimera_b200 import gpu
     if case == "field_loop_hlle_vl":
@@ -57,6 +58,9 @@ def test_tape_forward_is_the_fused_step(A, case):
     elif case == "generic_mixed_hlld":
         cfg, st = _generic_state(40, 3)            # x periodic, y outflow
         cfg = cfg.replace(riemann=HLLD, bc=(BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW))
+    elif case == "generic_pairs_hlld":
+        cfg, st = _generic_state(40, 4)            # a periodic side facing an outflow one, in x and in y
+        cfg = cfg.replace(riemann=HLLD, bc=(BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC))
     else:
         cfg, st = P.orszag_tang(48, riemann=RUSANOV, limiter=MC)
     s = gpu.Solver(cfg)
@@ -200,6 +204,10 @@ OUTFLOW_CASES = {
     "outflow_hlle_vl": dict(bc=(BC_OUTFLOW,) * 4),
     # x periodic, y outflow, HLLD + MC + MOOD
     "mixed_hlld_mc": dict(bc=(BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW), riemann=HLLD, limiter=MC),
+    # x = 0 periodic facing x = N outflow, y outflow, HLLE + Van Leer
+    "pair_xlo_periodic": dict(bc=(BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW, BC_OUTFLOW)),
+    # x = 0 outflow facing x = N periodic, y = 0 periodic facing y = N outflow, HLLD + MC + MOOD
+    "pairs_both_hlld_mc": dict(bc=(BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW), riemann=HLLD, limiter=MC),
 }
 
 
@@ -245,10 +253,12 @@ def test_adjoint_outflow_central_differences(A):
     _fd_check(A, cfg, st, nsteps=30, ndirs=6, K=10, seed=2, eps_rel=1e-7)
 
 
-def test_adjoint_rejects_a_periodic_side_paired_with_outflow(A):
-    cfg, _ = _generic_state(32, 1)
-    with pytest.raises(Exception):
-        A.Adjoint(cfg.replace(bc=(BC_PERIODIC, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC)))
+def test_adjoint_pairs_central_differences(A):
+    """A periodic side facing an outflow one in x and in y, HLLE + Van Leer,
+    30 steps: the adjoint against FP64 central differences, 1e-6 relative."""
+    cfg, st = _generic_state(64, 13)
+    cfg = cfg.replace(bc=(BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW))
+    _fd_check(A, cfg, st, nsteps=30, ndirs=6, K=10, seed=3, eps_rel=1e-7)
 
 
 def test_adjoint_checkpoint_interval_invariant(A):

@@ -6,8 +6,9 @@ outflow face N+1/2, whose right state is cell N itself; with x = 0 outflow
 and x = N periodic the face N+1/2 takes cell 1's reconstruction with the slope
 of its outflow ghost (src/mhd_derivatives.f90:148-161, 189-206).  The FP64
 handles run such grids through their own kernel instantiation and must match
-the FP64 oracle bit for bit, like every other boundary mix; the FP32 forms,
-the no-allocation step and the adjoint refuse them.
+the FP64 oracle bit for bit, like every other boundary mix (the adjoint's
+tests hold their own cases); the FP32 forms and the no-allocation step refuse
+them.
 """
 import numpy as np
 import pytest
