@@ -173,9 +173,6 @@ static int validate_cfg(const chimera_cfg* c) {
   if (c->limiter < 1 || c->limiter > 2) return CHIMERA_ERR_BAD_ARG;
   if (c->precision != CHIMERA_FP64 && c->precision != CHIMERA_FP32_BULK && c->precision != CHIMERA_FP32_MIXED)
     return CHIMERA_ERR_BAD_ARG;
-  // A side that wraps while its opposite side does not (a mixed pair; the
-  // reference takes each side on its own, src/mhd_bc.f90:45-100): FP64 only.
-  if (mixed_pair(*c) && c->precision != CHIMERA_FP64) return CHIMERA_ERR_UNSUPPORTED;
   return CHIMERA_OK;
 }
 
@@ -455,7 +452,9 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
   h->precision = cfgs[0].precision;
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  // a mixed pair in any member: the one tile compiled for it (FP64)
+  // a periodic side facing a non-periodic one (a mixed pair; the reference
+  // takes each side on its own, src/mhd_bc.f90:45-100) in any member: the one
+  // tile of the form compiled for it
   bool mixed = false;
   for (int m = 0; m < n_members; ++m) mixed = mixed || mixed_pair(cfgs[m]);
   const int nv = mixed                                 ? 1
@@ -464,7 +463,9 @@ int chimera_batch_create(int n_members, const chimera_cfg* cfgs, void* stream, c
                                                        : fp32m_variant_count();
   h->variants.resize(nv);
   for (int v = 0; v < nv; ++v) {
-    if (mixed) fp64_mixed_pair_kernels(&h->variants[v]);
+    if (mixed && h->precision == CHIMERA_FP64) fp64_mixed_pair_kernels(&h->variants[v]);
+    else if (mixed && h->precision == CHIMERA_FP32_BULK) fp32_mixed_pair_kernels(&h->variants[v]);
+    else if (mixed) fp32m_mixed_pair_kernels(&h->variants[v]);
     else if (h->precision == CHIMERA_FP64) fp64_kernels(v, &h->variants[v]);
     else if (h->precision == CHIMERA_FP32_BULK) fp32_kernels(v, &h->variants[v]);
     else fp32m_kernels(v, &h->variants[v]);

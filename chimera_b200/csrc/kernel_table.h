@@ -22,6 +22,8 @@ struct KernelSet {
 int fp64_variant_count();
 void fp64_kernels(int variant, KernelSet* out);
 void fp64_mixed_pair_kernels(KernelSet* out);
+void fp32_mixed_pair_kernels(KernelSet* out);
+void fp32m_mixed_pair_kernels(KernelSet* out);
 int fp32_variant_count();
 void fp32_kernels(int variant, KernelSet* out);
 int fp32m_variant_count();

@@ -10,14 +10,16 @@ namespace {
 // Storage type ST: float (FP32-bulk) or double (FP32 arithmetic on FP64
 // storage, whose CFL kernel has the FP64 epilogue's arithmetic; compiled in this
 // unit, its own instantiation).
-template <int TX, int TY, int NT, int MINB, bool SB = true, bool TMA = false, typename ST = float>
+template <int TX, int TY, int NT, int MINB, bool SB = true, bool TMA = false, typename ST = float,
+          bool MIXBC = false>
 void fill(KernelSet* ks) {
   using G = TileGeom32<TX, TY, SB>;
   const size_t smem = G::smem_bytes();
   const int bw = TMA ? G::BW : 0, bh = TMA ? G::BH : 0;
 #define CHIMERA_ENTRY(S, K)                                                                            \
   ks->stage[S - 1][K - 1] =                                                                           \
-      KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB, TMA, ST>, smem, TX, TY, NT, bw, bh}
+      KernelEntry{(const void*)&stage_kernel_f32<S, K, TX, TY, NT, MINB, SB, TMA, ST, MIXBC>, smem, TX, TY, NT, \
+                  bw, bh}
   CHIMERA_ENTRY(1, 1); CHIMERA_ENTRY(1, 2); CHIMERA_ENTRY(1, 3);
   CHIMERA_ENTRY(2, 1); CHIMERA_ENTRY(2, 2); CHIMERA_ENTRY(2, 3);
   CHIMERA_ENTRY(3, 1); CHIMERA_ENTRY(3, 2); CHIMERA_ENTRY(3, 3);
@@ -57,5 +59,9 @@ void fp32m_kernels(int variant, KernelSet* out) {
     default: fill<32, 16, 256, 2, true, false, double>(out); break;
   }
 }
+
+// The one tile of each form for grids with a periodic side facing a non-periodic one.
+void fp32_mixed_pair_kernels(KernelSet* out) { fill<32, 16, 256, 2, true, false, float, true>(out); }
+void fp32m_mixed_pair_kernels(KernelSet* out) { fill<32, 16, 256, 2, true, false, double, true>(out); }
 
 }  // namespace chimera

@@ -178,7 +178,8 @@ __device__ __forceinline__ void tma_issue(const StageArgs& a, int w, float* stg,
   for (int q = 0; q < 6; ++q) tma_load_2d(stg + q * BOXF, maps + q * TMAP_BYTES, i0 - 4, j0 - 3, bar);
 }
 
-template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB, bool TMA, typename S = float>
+template <int SOLVER, int STAGE, int TX, int TY, int NT, int MINB, bool SB, bool TMA, typename S = float,
+          bool MIXBC = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
   using G = TileGeom32<TX, TY, SB>;
   static_assert(!TMA || G::TMA_FITS, "TMA staging must fit in the slope arrays");
@@ -246,7 +247,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       continue;
     }
     const int nx = g.nx, ny = g.ny;
-    const int px = g.periodic_x, py = g.periodic_y;
+    const int px = g.periodic_x, py = g.periodic_y;                   // low sides
+    // high sides: they differ from the low sides only in a mixed pair (MIXBC
+    // instantiations), where a cell wrapped across the pair sees its neighbour
+    // across the non-periodic side as itself, as the cell it copies does
+    const int pxh = MIXBC ? g.periodic_xhi : px, pyh = MIXBC ? g.periodic_yhi : py;
     const int lt = w - g.tile_begin;
     const int i0 = (lt % g.tiles_x) * TX;
     const int j0 = (lt / g.tiles_x) * TY;
@@ -313,8 +318,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       for (int q = 0; q < 6; ++q) src[q] = reinterpret_cast<const S*>(g.buf[in_buf][q]);
       for (int p = tid; p < G::NP; p += NT) {
         const int qx = p % G::PX, qy = p / G::PX;
-        const int si = map_index(i0 - 2 + qx, nx, px, px);
-        const int sj = map_index(j0 - 2 + qy, ny, py, py);
+        const int si = map_index(i0 - 2 + qx, nx, px, pxh);
+        const int sj = map_index(j0 - 2 + qy, ny, py, pyh);
         const size_t idx = size_t(sj) * nx + si;
         const double bxc = src[4][idx], byc = src[5][idx];
         double Bx, By;
@@ -340,8 +345,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const int p = tid + k * NT;
         if (p < G::NP) {
           const int qx = p % G::PX, qy = p / G::PX;
-          const int si = map_index(i0 - 2 + qx, nx, px, px);
-          const int sj = map_index(j0 - 2 + qy, ny, py, py);
+          const int si = map_index(i0 - 2 + qx, nx, px, pxh);
+          const int sj = map_index(j0 - 2 + qy, ny, py, pyh);
           const size_t idx = size_t(sj) * nx + si;
           const size_t ixm = (si > 0) ? idx - 1 : (px ? idx + (nx - 1) : idx);
           const size_t iym = (sj > 0) ? idx - nx : (py ? idx + size_t(ny - 1) * nx : idx);
@@ -354,8 +359,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
         const int p = tid + k * NT;
         if (p < G::NP) {
           const int qx = p % G::PX, qy = p / G::PX;
-          const int si = map_index(i0 - 2 + qx, nx, px, px);
-          const int sj = map_index(j0 - 2 + qy, ny, py, py);
+          const int si = map_index(i0 - 2 + qx, nx, px, pxh);
+          const int sj = map_index(j0 - 2 + qy, ny, py, pyh);
           const S Bx = (si > 0 || px) ? S(0.5) * (ld[k][4] + ld[k][5]) : ld[k][4];
           const S By = (sj > 0 || py) ? S(0.5) * (ld[k][6] + ld[k][7]) : ld[k][6];
           const Prim<R> pr = get_primitive_mixed(ld[k][0], ld[k][1], ld[k][2], ld[k][3], Bx, By, g.gamma,
@@ -393,7 +398,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         const R* s = sP + q * G::NP;
-        const R f0 = s[pc], xm = s[pc - 1], xp = s[pc + 1], ym = s[pc - G::PX], yp = s[pc + G::PX];
+        R f0 = s[pc], xm = s[pc - 1], xp = s[pc + 1], ym = s[pc - G::PX], yp = s[pc + G::PX];
+        if constexpr (MIXBC) {
+          const int gx = i0 + cx - 1, gy = j0 + cy - 1;   // this cell, wrapped across a mixed pair?
+          if (px && !pxh && gx == -1) xp = f0;
+          if (!px && pxh && gx == nx) xm = f0;
+          if (py && !pyh && gy == -1) yp = f0;
+          if (!py && pyh && gy == ny) ym = f0;
+        }
         R sx, sy;
         if (slope_on) {
           if (van_leer) {
@@ -442,7 +454,15 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
             hi[q] = sHi[q * G::NS + c];
           } else {
             const R* s = sP + q * G::NP;
-            const R f0 = s[pa], xp = s[pa + 1], xm = s[pa - 1], yp = s[pa + G::PX], ym = s[pa - G::PX];
+            const R f0 = s[pa];
+            R xp = s[pa + 1], xm = s[pa - 1], yp = s[pa + G::PX], ym = s[pa - G::PX];
+            if constexpr (MIXBC) {
+              const int gx = i0 + cx - 1, gy = j0 + cy - 1;
+              if (px && !pxh && gx == -1) xp = f0;
+              if (!px && pxh && gx == nx) xm = f0;
+              if (py && !pyh && gy == -1) yp = f0;
+              if (!py && pyh && gy == ny) ym = f0;
+            }
             R l = fminf(fminf(fminf(fminf(f0, xp), xm), yp), ym);
             hi[q] = fmaxf(fmaxf(fmaxf(fmaxf(f0, xp), xm), yp), ym);
             if (q == 0 || q == 3) l = fmaxf(R(0.1e-8), l);
@@ -469,6 +489,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
                                       make_float2(f0, fp));
           R vL = v.x;
           R vR = v.y;
+          if constexpr (MIXBC) {
+            // the face below x = 0 (y = 0) with that side periodic and the far
+            // side outflow is the far side's outflow face: its high cell is the
+            // low cell's own ghost (value f0, zero slope)
+            const int gl = ydir ? j0 + cy - 1 : i0 + cx - 1;
+            if (gl == -1 && (ydir ? (py && !pyh) : (px && !pxh))) vR = f0;
+          }
           if (mood_on) {   // bounds of the LOW cell, reset to its value (src/mhd_derivatives.f90:213-216)
             if (vL < lo[q] || vL > hi[q]) { vL = f0; reset = true; }
             if (vR < lo[q] || vR > hi[q]) { vR = f0; reset = true; }
@@ -547,11 +574,16 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_f32(StageArgs a) {
       const int xi0 = (cj0 - j0 + 1) * G::FXW + (ci0 - i0 + 1), xi1 = (cj1 - j0 + 1) * G::FXW + (ci1 - i0 + 1);
       const int yi0 = (cj0 - j0 + 1) * G::FYW + (ci0 - i0 + 1), yi1 = (cj1 - j0 + 1) * G::FYW + (ci1 - i0 + 1);
       const R fa0 = FByX[xi0], fa1 = FByX[xi1];
-      const R up0 = (cj0 == ny - 1 && !py) ? fa0 : FByX[xi0 + G::FXW];
-      const R up1 = (cj1 == ny - 1 && !py) ? fa1 : FByX[xi1 + G::FXW];
+      // (also for the corner row below y = 0 that wraps to a non-periodic top: mixed pair)
+      const bool u0own = (cj0 == ny - 1 && !pyh) || (MIXBC && cj0 == -1 && py && !pyh);
+      const bool u1own = (cj1 == ny - 1 && !pyh) || (MIXBC && cj1 == -1 && py && !pyh);
+      const R up0 = u0own ? fa0 : FByX[xi0 + G::FXW];
+      const R up1 = u1own ? fa1 : FByX[xi1 + G::FXW];
       const R fb0 = FBxY[yi0], fb1 = FBxY[yi1];
-      const R rt0 = (ci0 == nx - 1 && !px) ? fb0 : FBxY[yi0 + 1];
-      const R rt1 = (ci1 == nx - 1 && !px) ? fb1 : FBxY[yi1 + 1];
+      const bool r0own = (ci0 == nx - 1 && !pxh) || (MIXBC && ci0 == -1 && px && !pxh);
+      const bool r1own = (ci1 == nx - 1 && !pxh) || (MIXBC && ci1 == -1 && px && !pxh);
+      const R rt0 = r0own ? fb0 : FBxY[yi0 + 1];
+      const R rt1 = r1own ? fb1 : FBxY[yi1 + 1];
       float2 t = __fadd2_rn(make_float2(-fa0, -fa1), make_float2(-up0, -up1));
       t = __fadd2_rn(t, make_float2(fb0, fb1));
       t = __fadd2_rn(t, make_float2(rt0, rt1));

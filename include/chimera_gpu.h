@@ -95,10 +95,9 @@ typedef struct chimera_handle chimera_handle;
 /* ---- single grid --------------------------------------------------------- */
 
 /* Create a solver for one grid.  stream: a cudaStream_t, or NULL to create one.
- * Each side takes its own boundary flag, as src/mhd_bc.f90:45-100 does; a
- * periodic side facing a non-periodic one is FP64 only (CHIMERA_ERR_UNSUPPORTED
- * for the FP32 forms).  Replaces the allocations of src/mhd_init.f90:99-164 for
- * the path's arrays. */
+ * Each side takes its own boundary flag, as src/mhd_bc.f90:45-100 does (a
+ * periodic side may face a non-periodic one, in every precision form).
+ * Replaces the allocations of src/mhd_init.f90:99-164 for the path's arrays. */
 int chimera_create(const chimera_cfg* cfg, void* stream, chimera_handle** out);
 
 /* Copy a conserved state in (host or device arrays); marks dt stale.  Host

@@ -59,7 +59,6 @@ def _cfg(**kw):
     (dict(gamma=1.0), -1),
     (dict(riemann=4), -1),
     (dict(limiter=0), -1),
-    (dict(bc=(1, 3, 1, 1), precision=1), -5),   # a periodic side facing a non-periodic one: FP64 only
     (dict(bc=(1, 1, 5, 5)), -1),
 ])
 def test_create_rejects_bad_config(lib, kw, code):
