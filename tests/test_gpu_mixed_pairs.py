@@ -15,7 +15,8 @@ import numpy as np
 import pytest
 
 from chimera_b200 import problems as P
-from chimera_b200.config import BC_OUTFLOW, BC_PERIODIC, FP32_BULK, FP32_MIXED, HLLD, HLLE, RUSANOV, VAN_LEER
+from chimera_b200.config import (BC_FIXED, BC_INFLOW, BC_OUTFLOW, BC_PERIODIC, FP32_BULK, FP32_MIXED, HLLD, HLLE,
+                                 RUSANOV, VAN_LEER)
 from tests.gpu_util import l1_rel, max_ulp, require_gpu
 
 pytestmark = pytest.mark.gpu
@@ -47,7 +48,16 @@ CASES = {
     "both_pairs_ragged": (lambda: _ragged((OUT, PER, PER, OUT)), 25),
     "no_slope_limiting": (lambda: (_ot(48, (OUT, PER, PER, OUT))[0].replace(slope_limiting=False),
                                    _ot(48, (OUT, PER, PER, OUT))[1]), 20),
+    # a grid smaller than one tile: halo positions wrap more than once
+    "tiny_8x6": (lambda: _small(8, 6, (PER, OUT, OUT, PER)), 20),
+    # fixed and inflow sides act as outflow (src/main.f90:349-354)
+    "fixed_inflow_sides": (lambda: _ot(40, (PER, BC_FIXED, BC_INFLOW, PER), riemann=HLLE), 20),
 }
+
+
+def _small(nx, ny, bc):
+    cfg, st = P.field_loop(nx, ny, 1.0, ny / nx, riemann=HLLE)
+    return cfg.replace(bc=bc), st
 
 
 @pytest.fixture(scope="module")
