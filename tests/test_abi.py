@@ -68,6 +68,20 @@ def test_create_rejects_bad_config(lib, kw, code):
     assert not h.value
 
 
+@pytest.mark.parametrize("precision", [0, 1, 2])
+@pytest.mark.parametrize("bc", [(1, 3, 1, 1), (3, 1, 2, 1), (1, 4, 3, 1)])
+def test_create_accepts_mixed_pairs(lib, precision, bc):
+    """A periodic side facing a non-periodic one passes the argument checks in
+    every precision form (the reference takes each side on its own): creation
+    succeeds on a GPU and stops at the device check without one."""
+    h = C.c_void_p()
+    cfg = _cfg(bc=bc, precision=precision)
+    rc = lib.chimera_create(C.byref(cfg), None, C.byref(h))
+    assert rc in (0, -6), rc
+    if rc == 0:
+        lib.chimera_destroy(h)
+
+
 def test_null_arguments(lib):
     h = C.c_void_p()
     assert lib.chimera_create(None, None, C.byref(h)) == -1
